@@ -1,0 +1,436 @@
+"""Benchmark of the sortArray path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+                    [--impl ours|reference]
+
+A step is one sortArray call over one batch of synthetic input (default:
+33,554,432 uint32 key + value pairs, keys = AND of two uniform draws masked to
+24 bits, value = index, bits [0, 24)). Each timed step starts from freshly
+restored input and a flushed L2 (a 256 MiB write between steps; the restore
+copy and the flush are outside the timed region). `value` is device-resident
+throughput in Mkeys/s over the K timed steps (CUDA events on the sort's
+stream, max over ranks); `e2e` is the same metric through the C ABI with
+pinned host buffers, host->device and device->host copies inside the timed
+region. The roofline entry is the onesweep pass kernel, whose launches are
+timed with CUDA events inside the same timed steps (sortEnableKernelTiming).
+
+Multi-GPU: the sort path does not shard (one global order), so N ranks run N
+independent replicas of the workload ("weak" scaling); the only collectives
+are the barrier and the max-over-ranks of the timings.
+
+--impl reference times the reference's CPU sort path on this host: the CPU
+radix sort of sort/src/cpusort/cpusort.cpp:122-186 as restated by the
+oracle (extended to values and bit ranges) on all host threads, over a
+bounded sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from mgpu_old_b200 import workloads  # noqa: E402
+
+METRIC = "sort Mkeys/s"
+UNIT = "Mkeys/s"
+FALLBACK_HBM_GBS = 6650.0
+CPU_SAMPLE = 1 << 22
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="pairs_and24_32M",
+                   choices=sorted(workloads.WORKLOADS))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_config(case, args, extra=None):
+    cfg = {"workload": case.name, "n": case.n, "value_count": case.value_count,
+           "first_bit": case.first_bit, "end_bit": case.end_bit,
+           "passes": len(_plan(case)), "parallelism": f"replicas{args.gpus}",
+           "l2": "flushed between steps (256 MiB write); inputs restored between steps"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def _plan(case):
+    from mgpu_old_b200 import api
+    return api.plan_passes(case.first_bit, case.end_bit)
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle's blocked LSD radix sort (cpusort.cpp:122-186 restated)
+
+
+def cpu_sort_sample(case, sample_n, threads):
+    """Time the oracle's multithreaded LSD sort on the first sample_n elements.
+    Returns seconds of one sort."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    keys = np.ascontiguousarray(case.keys[:sample_n])
+    vals = [np.ascontiguousarray(v[:sample_n]) for v in case.values]
+    bits = case.end_bit - case.first_bit
+    p = (bits + 7) // 8
+    widths = [bits // p + (i < bits % p) for i in range(p)]
+    t0 = time.perf_counter()
+    oracle.sort_lsd(keys, vals, case.value_count, case.first_bit, widths, 1 << 15, threads)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(case, budget_s=10.0):
+    threads = os.cpu_count() or 1
+    sample_n = min(case.n, CPU_SAMPLE)
+    total_t, total_n = 0.0, 0
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or total_n == 0:
+        total_t += cpu_sort_sample(case, sample_n, threads)
+        total_n += sample_n
+    return {"value": round(total_n / total_t / 1e6, 3), "unit": UNIT, "cores": threads,
+            "kind": "port",
+            "sample": f"first {sample_n} elements of {case.name}, oracle LSD radix "
+                      f"(cpusort.cpp:122-186 restated) on {threads} threads, "
+                      f"{total_n // sample_n} repetitions"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    case = workloads.WORKLOADS[args.workload]()
+    threads = os.cpu_count() or 1
+    sample_n = min(case.n, CPU_SAMPLE)
+    for _ in range(args.warmup):
+        cpu_sort_sample(case, sample_n, threads)
+    times = [cpu_sort_sample(case, sample_n, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = sample_n * len(times) / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total / len(times) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": workload_config(case, args, {"sample": sample_n}),
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads,
+                             "kind": "port",
+                             "sample": f"first {sample_n} elements per step"},
+            "e2e": {"value": round(value, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class GpuSorter:
+    """Device buffers for one workload plus a pristine copy to restore from."""
+
+    def __init__(self, case, device):
+        import torch
+        from mgpu_old_b200 import api
+        self.api = api
+        self.case = case
+        self.n = case.n
+        cap = (self.n + 2047) // 2048 * 2048
+        self.arrays = 1 if case.value_count == -1 else case.value_count
+
+        def dev(a):
+            t = torch.empty(cap, dtype=torch.int32, device=device)
+            t[:self.n] = torch.from_numpy(a.view(np.int32)).to(device)
+            return t
+
+        self.src_keys = dev(case.keys)
+        self.src_vals = [dev(v) for v in case.values]
+        self.bufs = {}
+        d = api.SortData()
+        d.maxElements, d.numElements, d.valueCount = cap, self.n, case.value_count
+        d.firstBit, d.endBit = case.first_bit, case.end_bit
+        for j in range(2):
+            t = torch.empty(cap, dtype=torch.int32, device=device)
+            self.bufs[t.data_ptr()] = t
+            d.keys[j] = t.data_ptr()
+        for i in range(self.arrays):
+            for j in range(2):
+                t = torch.empty(cap, dtype=torch.int32, device=device)
+                self.bufs[t.data_ptr()] = t
+                d.values[i][j] = t.data_ptr()
+        self.data = d
+        self.flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    def restore(self):
+        d = self.data
+        self.bufs[d.keys[0]][:self.n].copy_(self.src_keys[:self.n])
+        for i in range(len(self.src_vals)):
+            self.bufs[d.values[i][0]][:self.n].copy_(self.src_vals[i][:self.n])
+
+    def flush_l2(self):
+        self.flush_buf.zero_()
+
+    def result(self):
+        d = self.data
+        keys = self.bufs[d.keys[0]][:self.n].cpu().numpy().view(np.uint32)
+        vals = [self.bufs[d.values[i][0]][:self.n].cpu().numpy().view(np.uint32)
+                for i in range(self.arrays)]
+        return keys, vals
+
+
+def verify(case, keys, vals):
+    """Cheap full-size checks: field order, key multiset, and for index-valued
+    workloads the exact stable permutation."""
+    bits = case.end_bit - case.first_bit
+    mask = np.uint32(0xFFFFFFFF if bits >= 32 else (1 << bits) - 1)
+    f = (keys >> np.uint32(case.first_bit)) & mask
+    assert (f[1:] >= f[:-1]).all(), "output not ordered"
+    assert np.array_equal(np.sort(keys), np.sort(case.keys)), "keys not a permutation"
+    if case.value_count == 1 and np.array_equal(case.values[0][:16], np.arange(16)):
+        idx = vals[0]
+        assert np.array_equal(keys, case.keys[idx]), "values do not follow keys"
+        eq = f[1:] == f[:-1]
+        assert (idx[1:][eq] > idx[:-1][eq]).all(), "not stable"
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from mgpu_old_b200 import api
+    api.load_library()
+    case = workloads.WORKLOADS[args.workload]()
+    sorter = GpuSorter(case, device)
+    engine = api.MgpuSort()
+    d = sorter.data
+    stream = torch.cuda.current_stream(device)
+
+    def one_sort():
+        api.check(engine.sort_array(d))
+
+    # Warm-up.
+    for _ in range(max(args.warmup, 3)):
+        sorter.restore()
+        sorter.flush_l2()
+        one_sort()
+    api.check(engine.synchronize())
+    torch.cuda.synchronize()
+    keys, vals = sorter.result()
+    verify(case, keys, vals)
+
+    # Timed device-resident steps.
+    engine.enable_kernel_timing(True)
+    engine.read_kernel_timing()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        sorter.restore()
+        sorter.flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_sort()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    kt = engine.read_kernel_timing()
+    engine.enable_kernel_timing(False)
+    api.check(engine.synchronize())
+    keys, vals = sorter.result()
+    verify(case, keys, vals)
+
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+    value = case.n * world / (ms_per_step * 1e-3) / 1e6
+
+    # End to end through the C ABI with pinned host buffers.
+    pinned_in = [torch.from_numpy(case.keys.view(np.int32)).pin_memory()] + \
+        [torch.from_numpy(v.view(np.int32)).pin_memory() for v in case.values]
+    pinned_out = [torch.empty(case.n, dtype=torch.int32).pin_memory()
+                  for _ in range(1 + sorter.arrays)]
+    h2d = 4 * case.n * len(pinned_in)
+    d2h = 4 * case.n * len(pinned_out)
+    barrier()
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        sorter.flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sorter.bufs[d.keys[0]][:case.n].copy_(pinned_in[0], non_blocking=True)
+        for i in range(len(case.values)):
+            sorter.bufs[d.values[i][0]][:case.n].copy_(pinned_in[1 + i], non_blocking=True)
+        one_sort()
+        pinned_out[0].copy_(sorter.bufs[d.keys[0]][:case.n], non_blocking=True)
+        for i in range(sorter.arrays):
+            pinned_out[1 + i].copy_(sorter.bufs[d.values[i][0]][:case.n], non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    api.check(engine.synchronize())
+    verify(case, pinned_out[0].numpy().view(np.uint32),
+           [p.numpy().view(np.uint32) for p in pinned_out[1:]])
+    e2e_ms = max_over_ranks(e2e_ms)
+    e2e_value = case.n * world / (e2e_ms / args.steps * 1e-3) / 1e6
+
+    # Roofline of the onesweep pass kernel.
+    peak, peak_src = hbm_peak()
+    arrays = sorter.arrays
+    pass_bytes = 2 * case.n * 4 * (1 + arrays)
+    pass_launches = max(kt["pass_launches"], 1)
+    pass_ms = kt["pass_ms"] / pass_launches
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    alg_bytes = workloads.algorithmic_bytes(case.n, case.first_bit, case.end_bit,
+                                            case.value_count)
+    traffic = _ncu_traffic(case.name)
+    roofline = {"bound": "hbm", "kernel": "onesweep_kernel", "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_source": peak_src,
+                "traffic": traffic,
+                "bytes_per_launch": pass_bytes, "avg_launch_ms": round(pass_ms, 5),
+                "whole_sort": {"alg_bytes": alg_bytes,
+                               "achieved": round(alg_bytes / (ms_per_step * 1e-3) / 1e9, 1),
+                               "frac": round(alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak, 4)},
+                "upsweep_avg_ms": round(kt["upsweep_ms"] / max(kt["upsweep_launches"], 1), 5)}
+
+    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded numpy MT19937)",
+            "config": workload_config(case, args),
+            "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": kt["pass_launches"] + kt["upsweep_launches"],
+            "roofline": roofline,
+            "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(case)
+    engine.release()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def _ncu_traffic(workload):
+    """DRAM bytes per pass launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(workload)
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,648 @@
+// Host engine and C ABI of libmgpusort_b200.so.
+//
+// Follows the reference's host engine, sort/src/mgpusort/mgpusort.cpp: the
+// engine handle with its reference count (:200-261), sortData_d buffer
+// management (:655-734), the LSD pass loop with ping-pong swaps and parity
+// (:541-601), sortArray / sortArrayEx argument handling (:607-648) and the
+// sortHost / sortDevice conveniences (:740-806). The per-pass kernel chain
+// (:356-530) is replaced by one upsweep launch per sort and one onesweep
+// launch per pass (sort_kernels.cu).
+
+// The library is built with hidden visibility; the C ABI is all it exports.
+#pragma GCC visibility push(default)
+#include "../../include/mgpusort.h"
+#include "../../include/mgpusort_b200.h"
+#pragma GCC visibility pop
+#include "sort_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+// The struct layout callers compiled against (inc/mgpusort.h:63-147):
+// five ints, two bools, an int, then the pointer unions at offset 32.
+static_assert(offsetof(sortData_d, maxElements) == 0, "sortData_d layout");
+static_assert(offsetof(sortData_d, numElements) == 4, "sortData_d layout");
+static_assert(offsetof(sortData_d, valueCount) == 8, "sortData_d layout");
+static_assert(offsetof(sortData_d, firstBit) == 12, "sortData_d layout");
+static_assert(offsetof(sortData_d, endBit) == 16, "sortData_d layout");
+static_assert(offsetof(sortData_d, preserveEndKeys) == 20, "sortData_d layout");
+static_assert(offsetof(sortData_d, earlyExit) == 21, "sortData_d layout");
+static_assert(offsetof(sortData_d, parity) == 24, "sortData_d layout");
+static_assert(offsetof(sortData_d, keys) == 32, "sortData_d layout");
+static_assert(offsetof(sortData_d, values1) == 48, "sortData_d layout");
+static_assert(offsetof(sortData_d, values6) == 128, "sortData_d layout");
+static_assert(offsetof(sortData_d, pKeys) == 32, "sortData_d layout");
+static_assert(sizeof(sortData_d) == 144, "sortData_d layout");
+
+namespace {
+
+const char* const kStatusNames[] = {
+	"SORT_STATUS_SUCCESS",
+	"SORT_STATUS_NOT_INITIALIZED",
+	"SORT_STATUS_DEVICE_ALLOC_FAILED",
+	"SORT_STATUS_HOST_ALLOC_FAILED",
+	"SORT_STATUS_CONFIG_NOT_SUPPORTED",
+	"SORT_STATUS_CONTEXT_MISMATCH",
+	"SORT_STATUS_INVALID_CONTEXT",
+	"SORT_STATUS_KERNEL_NOT_FOUND",
+	"SORT_STATUS_KERNEL_ERROR",
+	"SORT_STATUS_LAUNCH_ERROR",
+	"SORT_STATUS_INVALID_VALUE",
+	"SORT_STATUS_DEVICE_ERROR",
+	"SORT_STATUS_INTERNAL_ERROR",
+	"SORT_STATUS_UNSUPPORTED_DEVICE"
+};
+
+// Buffer capacity granularity of library allocations, as in the reference
+// (mgpusort.cpp:663, 696).
+constexpr int kAllocRound = 2048;
+
+// Lookback epochs are 30 bits wide.
+constexpr unsigned kMaxEpoch = (1u << 30) - 1;
+
+int round_up(int x, int m) { return (int)(((long long)x + m - 1) / m * m); }
+
+} // namespace
+
+struct sortEngine_d {
+	long refs = 1;
+	int device = 0;
+	int numSMs = 0;
+	mgpusort::Control* ctrl = nullptr;
+	unsigned long long* status = nullptr;
+	size_t statusBytes = 0;
+	unsigned epoch = 0;
+	// Host-mapped error word written by kernels, read without synchronizing.
+	volatile unsigned* hostError = nullptr;
+	unsigned* hostErrorDev = nullptr;
+	// Pinned host copy of the trivial-pass flags (earlyExit read-back).
+	unsigned* hostTrivial = nullptr;
+	cudaEvent_t done = nullptr;
+	bool dirty = false;
+	int failTile = -1;
+	// Kernel timing (benchmarks): one event pair per timed launch.
+	struct TimedLaunch { cudaEvent_t start, stop; int kind; };
+	bool timing = false;
+	std::vector<TimedLaunch> timed;
+	size_t timedUsed = 0;
+};
+
+namespace {
+
+enum { kTimedUpsweep = 0, kTimedPass = 1 };
+
+// Opens a timed launch of `kind` on `stream`; returns its slot or -1.
+int timing_begin(sortEngine_d* e, int kind, cudaStream_t stream) {
+	if(!e->timing) return -1;
+	if(e->timedUsed == e->timed.size()) {
+		sortEngine_d::TimedLaunch t = {nullptr, nullptr, kind};
+		if(cudaEventCreate(&t.start) != cudaSuccess) return -1;
+		if(cudaEventCreate(&t.stop) != cudaSuccess) {
+			cudaEventDestroy(t.start);
+			return -1;
+		}
+		e->timed.push_back(t);
+	}
+	int slot = (int)e->timedUsed++;
+	e->timed[slot].kind = kind;
+	cudaEventRecord(e->timed[slot].start, stream);
+	return slot;
+}
+
+void timing_end(sortEngine_d* e, int slot, cudaStream_t stream) {
+	if(slot >= 0) cudaEventRecord(e->timed[slot].stop, stream);
+}
+
+// Release everything an engine holds; tolerates a partly built engine.
+void destroy_engine(sortEngine_d* e) {
+	if(!e) return;
+	if(e->done) cudaEventSynchronize(e->done);
+	for(auto& t : e->timed) {
+		cudaEventDestroy(t.start);
+		cudaEventDestroy(t.stop);
+	}
+	if(e->ctrl) cudaFree(e->ctrl);
+	if(e->status) cudaFree(e->status);
+	if(e->hostError) cudaFreeHost(const_cast<unsigned*>(e->hostError));
+	if(e->hostTrivial) cudaFreeHost(e->hostTrivial);
+	if(e->done) cudaEventDestroy(e->done);
+	delete e;
+}
+
+// sortArray's plan: the fewest passes of at most 8 bits, widths balanced
+// (wider passes first), least significant digit first.
+int plan_widths_default(int numBits, int* widths) {
+	int passes = (numBits + 7) / 8;
+	for(int p = 0; p < passes; ++p)
+		widths[p] = numBits / passes + (p < numBits % passes ? 1 : 0);
+	return passes;
+}
+
+// sortArrayEx's plan, as the reference builds it (mgpusort.cpp:626-646 and
+// the table walk of :574-576): ceil(bits / bitPass) passes, `split` of them
+// one bit narrower, the narrower ones first.
+int plan_widths_reference(int numBits, int bitPass, int* widths) {
+	if(bitPass <= 0 || bitPass > 6) bitPass = 6;
+	if(bitPass > numBits) bitPass = numBits;
+	int passes = (numBits + bitPass - 1) / bitPass;
+	int split = passes * bitPass - numBits;
+	for(int p = 0; p < passes; ++p) widths[p] = bitPass - (p < split ? 1 : 0);
+	return passes;
+}
+
+bool make_plan(int firstBit, int numBits, int bitPass, mgpusort::PassPlan* plan) {
+	int widths[mgpusort::kMaxPasses];
+	int passes = bitPass ? plan_widths_reference(numBits, bitPass, widths)
+		: plan_widths_default(numBits, widths);
+	if(passes > mgpusort::kMaxPasses) return false;
+	std::memset(plan, 0, sizeof(*plan));
+	plan->numPasses = passes;
+	int bit = firstBit, bin = 0;
+	for(int p = 0; p < passes; ++p) {
+		plan->shift[p] = bit;
+		plan->width[p] = widths[p];
+		plan->binBase[p] = bin;
+		bit += widths[p];
+		bin += 1 << widths[p];
+	}
+	plan->totalBins = bin;
+	return bin <= mgpusort::kMaxBins;
+}
+
+bool aligned16(CUdeviceptr p) { return (p & 15) == 0; }
+
+// Checks the status of a launch sequence.
+sortStatus_t launch_status(cudaError_t e) {
+	if(e == cudaSuccess) return SORT_STATUS_SUCCESS;
+	return SORT_STATUS_LAUNCH_ERROR;
+}
+
+sortStatus_t take_device_error(sortEngine_d* e) {
+	unsigned err = *e->hostError;
+	if(!err) return SORT_STATUS_SUCCESS;
+	*e->hostError = 0;
+	e->dirty = true;
+	return SORT_STATUS_KERNEL_ERROR;
+}
+
+sortStatus_t ensure_status(sortEngine_d* e, size_t bytes) {
+	if(bytes <= e->statusBytes) return SORT_STATUS_SUCCESS;
+	// Grow only (like the reference's scratch, mgpusort.cpp:319-343). The
+	// old buffer may still be read by queued work: cudaFree waits for it.
+	if(e->status) cudaFree(e->status);
+	e->status = nullptr;
+	e->statusBytes = 0;
+	void* p = nullptr;
+	if(cudaMalloc(&p, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_DEVICE_ALLOC_FAILED;
+	}
+	// Fresh memory may hold any bits; epoch 0 is never used by a pass.
+	if(cudaMemset(p, 0, bytes) != cudaSuccess) {
+		cudaFree(p);
+		return SORT_STATUS_DEVICE_ERROR;
+	}
+	e->status = static_cast<unsigned long long*>(p);
+	e->statusBytes = bytes;
+	return SORT_STATUS_SUCCESS;
+}
+
+unsigned next_epoch(sortEngine_d* e, cudaStream_t stream) {
+	if(e->epoch >= kMaxEpoch) {
+		cudaMemsetAsync(e->status, 0, e->statusBytes, stream);
+		e->epoch = 0;
+	}
+	return ++e->epoch;
+}
+
+void swap_buffers(sortData_d* d) {
+	std::swap(d->keys[0], d->keys[1]);
+	for(int i = 0; i < 6; ++i) std::swap(d->values[i][0], d->values[i][1]);
+	d->parity ^= 1;
+}
+
+// The whole sort of one sortData_d: validation, upsweep, the pass loop.
+// bitPass 0 selects sortArray's plan, 1..6 sortArrayEx's.
+sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
+	cudaStream_t stream) {
+	if(!e || !d) return SORT_STATUS_INVALID_VALUE;
+	sortStatus_t pending = take_device_error(e);
+	if(pending != SORT_STATUS_SUCCESS) return pending;
+
+	const int numBits = d->endBit - d->firstBit;
+	if(!numBits) return SORT_STATUS_SUCCESS;   // mgpusort.cpp:610
+	if(numBits < 0 || numBits > 32 || d->firstBit < 0 || d->endBit > 32)
+		return SORT_STATUS_INVALID_VALUE;
+	if(d->numElements > d->maxElements || d->numElements < 0)
+		return SORT_STATUS_INVALID_VALUE;
+	if(d->valueCount < -1 || d->valueCount > 6) return SORT_STATUS_INVALID_VALUE;
+
+	const int n = d->numElements;
+	const bool indexMode = d->valueCount == -1;
+	const int numArrays = indexMode ? 1 : d->valueCount;
+	if(!d->keys[0] || !d->keys[1]) return SORT_STATUS_INVALID_VALUE;
+	for(int i = 0; i < numArrays; ++i)
+		if(!d->values[i][0] || !d->values[i][1]) return SORT_STATUS_INVALID_VALUE;
+	if(!n) return SORT_STATUS_SUCCESS;
+
+	mgpusort::PassPlan plan;
+	if(!make_plan(d->firstBit, numBits, bitPass, &plan))
+		return SORT_STATUS_INTERNAL_ERROR;
+
+	size_t statusBytes = mgpusort::pass_status_bytes(n, numArrays);
+	if(indexMode)
+		statusBytes = std::max(statusBytes,
+			mgpusort::pass_status_bytes(n, mgpusort::kValueIndex));
+	sortStatus_t st = ensure_status(e, statusBytes);
+	if(st != SORT_STATUS_SUCCESS) return st;
+
+	if(e->dirty) {
+		if(cudaMemsetAsync(e->ctrl, 0, sizeof(mgpusort::Control), stream)
+			!= cudaSuccess) return SORT_STATUS_DEVICE_ERROR;
+		e->dirty = false;
+	}
+
+	bool bulk = true;
+	for(int i = 0; i < 2; ++i) bulk = bulk && aligned16(d->keys[i]);
+	for(int i = 0; i < numArrays; ++i)
+		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
+
+	int slot = timing_begin(e, kTimedUpsweep, stream);
+	cudaError_t ce = mgpusort::launch_upsweep(
+		reinterpret_cast<const unsigned*>(d->keys[0]), n, plan, e->ctrl,
+		e->hostErrorDev, e->numSMs, stream);
+	timing_end(e, slot, stream);
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+
+	// earlyExit: one read-back of the per-pass "single digit" flags, then
+	// skip those passes (the reference reads its detect counters back per
+	// pass for the same purpose, mgpusort.cpp:434-451).
+	bool skip[mgpusort::kMaxPasses] = {};
+	if(d->earlyExit) {
+		if(cudaMemcpyAsync(e->hostTrivial, e->ctrl->trivial,
+			sizeof(unsigned) * plan.numPasses, cudaMemcpyDeviceToHost, stream)
+			!= cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
+			e->dirty = true;
+			return SORT_STATUS_DEVICE_ERROR;
+		}
+		for(int p = 0; p < plan.numPasses; ++p) skip[p] = e->hostTrivial[p] != 0;
+	}
+
+	bool firstExecuted = true;
+	for(int p = 0; p < plan.numPasses; ++p) {
+		if(skip[p]) continue;
+		const int vm = (indexMode && firstExecuted) ? mgpusort::kValueIndex
+			: numArrays;
+		mgpusort::PassBuffers buf = {};
+		buf.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
+		buf.keysOut = reinterpret_cast<unsigned*>(d->keys[1]);
+		for(int i = 0; i < 6; ++i) {
+			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
+			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
+		}
+		const unsigned epoch = next_epoch(e, stream);
+		slot = timing_begin(e, kTimedPass, stream);
+		ce = mgpusort::launch_pass(buf, vm, n, p, plan, e->ctrl, e->status,
+			epoch, bulk, e->failTile, e->hostErrorDev, stream);
+		timing_end(e, slot, stream);
+		e->failTile = -1;
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+		swap_buffers(d);
+		firstExecuted = false;
+	}
+	if(indexMode && firstExecuted) {
+		// Every pass was skipped: the identity order still needs its indices.
+		ce = mgpusort::launch_iota(reinterpret_cast<unsigned*>(d->values1[0]), n,
+			stream);
+		if(ce != cudaSuccess) return launch_status(ce);
+	}
+	cudaEventRecord(e->done, stream);
+	return SORT_STATUS_SUCCESS;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* SORTAPI sortStatusString(sortStatus_t status) {
+	int code = (int)status;
+	if(code < 0 || code >= (int)(sizeof(kStatusNames) / sizeof(kStatusNames[0])))
+		return nullptr;
+	return kStatusNames[code];
+}
+
+sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
+	sortEngine_t* engine) {
+	(void)kernelPath;
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	*engine = nullptr;
+	int device = 0;
+	if(cudaGetDevice(&device) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_INVALID_CONTEXT;
+	}
+	cudaDeviceProp prop;
+	if(cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_INVALID_CONTEXT;
+	}
+	if(prop.major != 10 || prop.minor != 0) return SORT_STATUS_UNSUPPORTED_DEVICE;
+
+	sortEngine_d* e = new sortEngine_d;
+	e->device = device;
+	e->numSMs = prop.multiProcessorCount;
+	sortStatus_t status = SORT_STATUS_SUCCESS;
+	void* p = nullptr;
+	if(mgpusort::configure_kernels() != cudaSuccess)
+		status = SORT_STATUS_KERNEL_ERROR;
+	else if(cudaMalloc(&p, sizeof(mgpusort::Control)) != cudaSuccess)
+		status = SORT_STATUS_DEVICE_ALLOC_FAILED;
+	else {
+		e->ctrl = static_cast<mgpusort::Control*>(p);
+		if(cudaMemset(e->ctrl, 0, sizeof(mgpusort::Control)) != cudaSuccess)
+			status = SORT_STATUS_DEVICE_ERROR;
+	}
+	if(status == SORT_STATUS_SUCCESS) {
+		void* h = nullptr;
+		if(cudaHostAlloc(&h, sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess)
+			status = SORT_STATUS_HOST_ALLOC_FAILED;
+		else {
+			e->hostError = static_cast<unsigned*>(h);
+			*e->hostError = 0;
+			void* dp = nullptr;
+			if(cudaHostGetDevicePointer(&dp, h, 0) != cudaSuccess)
+				status = SORT_STATUS_HOST_ALLOC_FAILED;
+			e->hostErrorDev = static_cast<unsigned*>(dp);
+		}
+	}
+	if(status == SORT_STATUS_SUCCESS) {
+		void* h = nullptr;
+		if(cudaHostAlloc(&h, sizeof(unsigned) * mgpusort::kMaxPasses,
+			cudaHostAllocDefault) != cudaSuccess)
+			status = SORT_STATUS_HOST_ALLOC_FAILED;
+		e->hostTrivial = static_cast<unsigned*>(h);
+	}
+	if(status == SORT_STATUS_SUCCESS &&
+		cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess)
+		status = SORT_STATUS_DEVICE_ERROR;
+	if(status != SORT_STATUS_SUCCESS) {
+		cudaGetLastError();
+		destroy_engine(e);
+		return status;
+	}
+	*engine = e;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortLoadKernel(sortEngine_t engine, int numSortThreads,
+	int valuesPerThread, bool useTransList, int valueCount) {
+	(void)useTransList;
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	// The reference's checks (mgpusort.cpp:148-153).
+	if(numSortThreads != 128 && numSortThreads != 256)
+		return SORT_STATUS_INVALID_VALUE;
+	if(valuesPerThread != 4 && valuesPerThread != 8)
+		return SORT_STATUS_INVALID_VALUE;
+	if(valueCount < -1 || valueCount > 6) return SORT_STATUS_INVALID_VALUE;
+	return mgpusort::configure_kernels() == cudaSuccess ? SORT_STATUS_SUCCESS
+		: SORT_STATUS_KERNEL_ERROR;
+}
+
+sortStatus_t SORTAPI sortIncEngine(sortEngine_t engine) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	++engine->refs;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortReleaseEngine(sortEngine_t engine) {
+	if(engine && !--engine->refs) destroy_engine(engine);
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortCreateData(sortEngine_t engine, int maxElements,
+	int valueCount, sortData_t* data) {
+	if(!data || valueCount > 6 || valueCount < -1 || maxElements < 0)
+		return SORT_STATUS_INVALID_VALUE;
+	sortData_d* d = new sortData_d;
+	std::memset(d, 0, sizeof(*d));
+	d->maxElements = round_up(maxElements, kAllocRound);
+	d->numElements = maxElements;
+	d->valueCount = valueCount;
+	d->firstBit = 0;
+	d->endBit = 32;
+	sortStatus_t status = sortAllocData(engine, d);
+	if(status != SORT_STATUS_SUCCESS) {
+		sortFreeData(d);
+		delete d;
+		*data = nullptr;
+		return status;
+	}
+	*data = d;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortDestroyData(sortData_t data) {
+	if(!data) return SORT_STATUS_SUCCESS;
+	sortFreeData(data);
+	delete data;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortAllocData(sortEngine_t engine, sortData_t data) {
+	(void)engine;
+	if(!data || data->valueCount > 6 || data->valueCount < -1 ||
+		data->maxElements < 0) return SORT_STATUS_INVALID_VALUE;
+	const size_t elems = (size_t)round_up(data->maxElements, kAllocRound);
+	const int count = data->valueCount == -1 ? 1 : data->valueCount;
+	// keys[0], keys[1], values1[0], values1[1], ... are consecutive.
+	CUdeviceptr* slots = data->keys;
+	CUdeviceptr fresh[14] = {};
+	for(int i = 0; i < 2 + 2 * count; ++i) {
+		if(slots[i]) continue;
+		void* p = nullptr;
+		if(elems && cudaMalloc(&p, elems * sizeof(unsigned)) != cudaSuccess) {
+			cudaGetLastError();
+			for(int j = 0; j < i; ++j)
+				if(fresh[j]) cudaFree(reinterpret_cast<void*>(fresh[j]));
+			return SORT_STATUS_DEVICE_ALLOC_FAILED;
+		}
+		fresh[i] = reinterpret_cast<CUdeviceptr>(p);
+	}
+	for(int i = 0; i < 2 + 2 * count; ++i)
+		if(fresh[i]) slots[i] = fresh[i];
+	data->parity = 0;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortFreeData(sortData_d* data) {
+	if(!data) return SORT_STATUS_INVALID_VALUE;
+	for(int i = 0; i < 2; ++i) {
+		if(data->keys[i]) cudaFree(reinterpret_cast<void*>(data->keys[i]));
+		for(int j = 0; j < 6; ++j)
+			if(data->values[j][i])
+				cudaFree(reinterpret_cast<void*>(data->values[j][i]));
+	}
+	std::memset(data, 0, sizeof(*data));
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortArray(sortEngine_t engine, sortData_t data) {
+	return sort_impl(engine, data, 0, cudaStreamLegacy);
+}
+
+sortStatus_t SORTAPI sortArrayEx(sortEngine_t engine, sortData_t data,
+	int numSortThreads, int valuesPerThread, int bitPass, bool useTransList) {
+	(void)useTransList;
+	if(!data) return SORT_STATUS_INVALID_VALUE;
+	// mgpusort.cpp:621-626.
+	if((numSortThreads != 128 && numSortThreads != 256) || valuesPerThread != 8)
+		return SORT_STATUS_INVALID_VALUE;
+	if(data->numElements > data->maxElements) return SORT_STATUS_INVALID_VALUE;
+	if(bitPass <= 0 || bitPass > 6) bitPass = 6;
+	return sort_impl(engine, data, bitPass, cudaStreamLegacy);
+}
+
+sortStatus_t SORTAPI sortArrayAsync(sortEngine_t engine, sortData_t data,
+	CUstream stream) {
+	return sort_impl(engine, data, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+sortStatus_t SORTAPI sortSynchronize(sortEngine_t engine) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	if(cudaEventSynchronize(engine->done) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_DEVICE_ERROR;
+	}
+	return take_device_error(engine);
+}
+
+int SORTAPI sortPlanPasses(int firstBit, int endBit, int bitPass,
+	int* widths) {
+	const int numBits = endBit - firstBit;
+	if(firstBit < 0 || endBit > 32 || numBits < 0 || !widths) return -1;
+	if(!numBits) return 0;
+	if(bitPass < 0 || bitPass > 6) return -1;
+	return bitPass ? plan_widths_reference(numBits, bitPass, widths)
+		: plan_widths_default(numBits, widths);
+}
+
+sortStatus_t SORTAPI sortInjectFault(sortEngine_t engine, int tile) {
+	if(!engine || tile < -1) return SORT_STATUS_INVALID_VALUE;
+	engine->failTile = tile;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	engine->timing = enable != 0;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
+	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	double ms[2] = {0, 0};
+	int launches[2] = {0, 0};
+	sortStatus_t status = SORT_STATUS_SUCCESS;
+	for(size_t i = 0; i < engine->timedUsed; ++i) {
+		auto& t = engine->timed[i];
+		float f = 0;
+		if(cudaEventSynchronize(t.stop) != cudaSuccess ||
+			cudaEventElapsedTime(&f, t.start, t.stop) != cudaSuccess) {
+			cudaGetLastError();
+			status = SORT_STATUS_DEVICE_ERROR;
+			continue;
+		}
+		ms[t.kind] += f;
+		++launches[t.kind];
+	}
+	engine->timedUsed = 0;
+	if(upsweepMs) *upsweepMs = ms[kTimedUpsweep];
+	if(upsweepLaunches) *upsweepLaunches = launches[kTimedUpsweep];
+	if(passMs) *passMs = ms[kTimedPass];
+	if(passLaunches) *passLaunches = launches[kTimedPass];
+	return status;
+}
+
+sortStatus_t SORTAPI sortHost(sortEngine_t engine, unsigned int* keys,
+	unsigned int* values, int numElements, int numBits) {
+	if(!engine || !keys || numElements < 0 || numBits < 0 || numBits > 32)
+		return SORT_STATUS_INVALID_VALUE;
+	if(!numElements) return SORT_STATUS_SUCCESS;
+	sortData_d d;
+	std::memset(&d, 0, sizeof(d));
+	d.maxElements = numElements;
+	d.numElements = numElements;
+	d.valueCount = values ? 1 : 0;
+	d.endBit = numBits;
+	sortStatus_t status = sortAllocData(engine, &d);
+	if(status != SORT_STATUS_SUCCESS) return status;
+	const size_t bytes = sizeof(unsigned) * (size_t)numElements;
+	if(cudaMemcpy(reinterpret_cast<void*>(d.keys[0]), keys, bytes,
+		cudaMemcpyHostToDevice) != cudaSuccess ||
+		(values && cudaMemcpy(reinterpret_cast<void*>(d.values1[0]), values,
+			bytes, cudaMemcpyHostToDevice) != cudaSuccess))
+		status = SORT_STATUS_DEVICE_ERROR;
+	if(status == SORT_STATUS_SUCCESS) status = sortArray(engine, &d);
+	if(status == SORT_STATUS_SUCCESS) {
+		if(cudaMemcpy(keys, reinterpret_cast<void*>(d.keys[0]), bytes,
+			cudaMemcpyDeviceToHost) != cudaSuccess ||
+			(values && cudaMemcpy(values, reinterpret_cast<void*>(d.values1[0]),
+				bytes, cudaMemcpyDeviceToHost) != cudaSuccess))
+			status = SORT_STATUS_DEVICE_ERROR;
+	}
+	if(status == SORT_STATUS_SUCCESS) status = sortSynchronize(engine);
+	cudaGetLastError();
+	sortFreeData(&d);
+	return status;
+}
+
+sortStatus_t SORTAPI sortDevice(sortEngine_t engine, CUdeviceptr keys,
+	CUdeviceptr values, int numElements, int numBits) {
+	if(!engine || !keys || numElements < 0 || numBits < 0 || numBits > 32)
+		return SORT_STATUS_INVALID_VALUE;
+	if(!numElements) return SORT_STATUS_SUCCESS;
+	sortData_d d;
+	std::memset(&d, 0, sizeof(d));
+	d.keys[0] = keys;
+	d.values1[0] = values;
+	d.maxElements = numElements;
+	d.numElements = numElements;
+	d.valueCount = values ? 1 : 0;
+	d.endBit = numBits;
+	sortStatus_t status = sortAllocData(engine, &d);
+	if(status != SORT_STATUS_SUCCESS) return status;
+	status = sortArray(engine, &d);
+	const size_t bytes = sizeof(unsigned) * (size_t)numElements;
+	if(status == SORT_STATUS_SUCCESS && d.keys[0] != keys) {
+		// An odd number of passes: the result is in the library's buffer.
+		if(cudaMemcpyAsync(reinterpret_cast<void*>(keys),
+			reinterpret_cast<void*>(d.keys[0]), bytes, cudaMemcpyDeviceToDevice,
+			cudaStreamLegacy) != cudaSuccess ||
+			(values && cudaMemcpyAsync(reinterpret_cast<void*>(values),
+				reinterpret_cast<void*>(d.values1[0]), bytes,
+				cudaMemcpyDeviceToDevice, cudaStreamLegacy) != cudaSuccess))
+			status = SORT_STATUS_DEVICE_ERROR;
+	}
+	if(status == SORT_STATUS_SUCCESS) {
+		if(cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess)
+			status = SORT_STATUS_DEVICE_ERROR;
+		else status = take_device_error(engine);
+	}
+	cudaGetLastError();
+	// Free only the library's buffers.
+	for(int i = 0; i < 2; ++i) {
+		if(d.keys[i] == keys) d.keys[i] = 0;
+		if(d.values1[i] == values) d.values1[i] = 0;
+	}
+	sortFreeData(&d);
+	return status;
+}
+
+} // extern "C"

@@ -1,0 +1,80 @@
+// Host-visible interface of the sort kernels (sort_kernels.cu): the device
+// control block, the pass plan and the launchers the engine calls.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace mgpusort {
+
+// A pass sorts by a digit of at most 8 bits; a 32-bit range needs at most 32
+// passes (sortArrayEx with bitPass = 1) and the digit histograms of all
+// passes of one plan take at most 4 * 256 bins.
+constexpr int kMaxPasses = 32;
+constexpr int kMaxBins = 1024;
+constexpr int kDigitBins = 256;
+
+// Device control block, one per engine. The upsweep adds every key's digits
+// into hist, and its last CTA turns hist into the exclusive offsets, sets
+// trivial[p] when pass p has a single non-empty digit, and zeroes hist and
+// ticket again. Each pass kernel draws tile ids from tileCounter[p]; the CTA
+// that draws the last id re-arms the counter. So the block is clean after
+// every complete sort and needs a memset only after an error.
+struct Control {
+	unsigned hist[kMaxBins];
+	unsigned offsets[kMaxBins];
+	unsigned trivial[kMaxPasses];
+	unsigned tileCounter[kMaxPasses];
+	unsigned ticket;
+	unsigned error;
+	unsigned reserved[62];
+};
+
+// Digit layout of a sort: pass p sorts by bits [shift[p], shift[p] +
+// width[p]) and its histogram lives at hist[binBase[p] .. + 2^width[p]).
+struct PassPlan {
+	int numPasses;
+	int shift[kMaxPasses];
+	int width[kMaxPasses];
+	int binBase[kMaxPasses];
+	int totalBins;
+};
+
+// One pass reads keysIn (and valsIn[0..v)) and writes keysOut (valsOut).
+struct PassBuffers {
+	const unsigned* keysIn;
+	unsigned* keysOut;
+	const unsigned* valsIn[6];
+	unsigned* valsOut[6];
+};
+
+// Value modes of a pass: -1 writes each key's source position into
+// valsOut[0] (index mode, first pass), 0 moves keys only, 1..6 moves that many
+// value arrays with the keys.
+constexpr int kValueIndex = -1;
+
+// Elements per tile of the pass kernel for a value mode.
+int pass_tile_elements(int valueMode);
+
+// Bytes of lookback status needed for a pass over n elements.
+size_t pass_status_bytes(int n, int valueMode);
+
+// Configure kernel attributes (dynamic shared memory); call once per device.
+cudaError_t configure_kernels();
+
+cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
+	Control* ctrl, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream);
+
+// useBulk: every buffer of the pass is 16-byte aligned, so full tiles are
+// staged with bulk copies; otherwise every tile uses plain loads.
+// failTile >= 0 makes that tile skip its lookback publication (fault
+// injection for tests of the bounded waits); -1 in normal use.
+cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, Control* ctrl,
+	unsigned long long* status, unsigned epoch, bool useBulk, int failTile,
+	volatile unsigned* hostError, cudaStream_t stream);
+
+cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream);
+
+} // namespace mgpusort

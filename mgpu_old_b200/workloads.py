@@ -1,0 +1,83 @@
+"""Seeded synthetic inputs for the sort workloads (numpy, host memory).
+
+Each generator returns host arrays of the workload's shape and value
+distribution. There is no public dataset for this path; these stand in for
+the reference's own benchmark inputs (uniform random keys, value = index,
+sort/src/testsort/testsort.cpp:176-194).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class SortCase:
+    name: str
+    keys: np.ndarray
+    values: list[np.ndarray] = field(default_factory=list)
+    value_count: int = 0          # -1 index mode, 0 keys only, 1..6
+    first_bit: int = 0
+    end_bit: int = 32
+
+    @property
+    def n(self) -> int:
+        return int(self.keys.size)
+
+
+def _rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.MT19937(seed))
+
+
+def _u32(rng: np.random.Generator, n: int, high: int = 1 << 32) -> np.ndarray:
+    return rng.integers(0, high, size=n, dtype=np.uint64).astype(np.uint32)
+
+
+def keys_uniform32(n: int = 1 << 20, seed: int = 1) -> SortCase:
+    """Keys-only, uniform over 32 bits, [0, 32). 1,048,576 keys by default."""
+    return SortCase("keys_u32_1M" if n == 1 << 20 else f"keys_u32_{n}",
+                    _u32(_rng(seed), n))
+
+
+def pairs_and24(n: int = 1 << 25, seed: int = 2) -> SortCase:
+    """Key-value: key = (r1 & r2) & 0xFFFFFF (skewed digits), value = index,
+    bits [0, 24). 33,554,432 pairs by default."""
+    rng = _rng(seed)
+    keys = (_u32(rng, n) & _u32(rng, n)) & np.uint32(0x00FFFFFF)
+    return SortCase("pairs_and24_32M" if n == 1 << 25 else f"pairs_and24_{n}",
+                    keys, [np.arange(n, dtype=np.uint32)], 1, 0, 24)
+
+
+def multi6_17bit(n: int = 1 << 24, seed: int = 3) -> SortCase:
+    """Key + 6 value arrays: keys uniform in [0, 2^17) (heavy duplicates),
+    random payloads, full 32-bit range. 16,777,216 keys by default."""
+    rng = _rng(seed)
+    keys = _u32(rng, n, 1 << 17)
+    vals = [_u32(rng, n) for _ in range(6)]
+    return SortCase("multi6_17bit_16M" if n == 1 << 24 else f"multi6_17bit_{n}",
+                    keys, vals, 6, 0, 32)
+
+
+def pairs_uniform32(n: int = 1 << 26, seed: int = 5) -> SortCase:
+    """Key-value, uniform 32-bit keys, value = index, [0, 32). 64M pairs."""
+    rng = _rng(seed)
+    return SortCase("pairs_u32_64M" if n == 1 << 26 else f"pairs_u32_{n}",
+                    _u32(rng, n), [np.arange(n, dtype=np.uint32)], 1, 0, 32)
+
+
+WORKLOADS = {
+    "keys_u32_1M": keys_uniform32,
+    "pairs_and24_32M": pairs_and24,
+    "multi6_17bit_16M": multi6_17bit,
+    "pairs_u32_64M": pairs_uniform32,
+}
+
+
+def algorithmic_bytes(n: int, first_bit: int, end_bit: int, value_count: int) -> int:
+    """Canonical bytes of a sort: one key read for the histograms plus, per
+    8-bit pass, one read and one write of every key and value:
+    N * (4 + 2 * P * (4 + 4V)), P = ceil(bits / 8), index mode V = 1."""
+    p = (end_bit - first_bit + 7) // 8
+    v = 1 if value_count == -1 else value_count
+    return n * (4 + 2 * p * (4 + 4 * v))
