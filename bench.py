@@ -49,12 +49,14 @@ CPU_SAMPLE = 1 << 22
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="pairs_and24_32M",
                    choices=sorted(workloads.WORKLOADS))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-only", action="store_true",
+                   help="warm-up plus --steps sorts, no e2e/CPU legs (for ncu)")
     return p.parse_args()
 
 
@@ -159,6 +161,7 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Start sampling; returns once the first sample arrived (or 10 s)."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
@@ -168,6 +171,18 @@ class ClockSampler:
             self.thread.start()
         except Exception:
             self.proc = None
+            return
+        t_end = time.time() + 10
+        while not self.lines and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.first = len(self.lines)
+
+    def wait_one_more(self):
+        """Block until at least one sample was taken after start()."""
+        t_end = time.time() + 5
+        while self.proc and len(self.lines) <= getattr(self, "first", 0) \
+                and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -176,6 +191,7 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return None
+        self.wait_one_more()
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -184,7 +200,7 @@ class ClockSampler:
         self.thread.join(timeout=5)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[max(getattr(self, "first", 1) - 1, 0):]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -318,6 +334,16 @@ def main():
     torch.cuda.synchronize()
     keys, vals = sorter.result()
     verify(case, keys, vals)
+
+    if args.profile_only:
+        for _ in range(args.steps):
+            sorter.restore()
+            sorter.flush_l2()
+            one_sort()
+        api.check(engine.synchronize())
+        torch.cuda.synchronize()
+        engine.release()
+        return 0
 
     # Timed device-resident steps.
     engine.enable_kernel_timing(True)

@@ -62,7 +62,7 @@ __device__ __forceinline__ void count_digits(unsigned* hist,
 	if(run) atomicAdd(&hist[cur], run);
 }
 
-__global__ void __launch_bounds__(kUpThreads) upsweep_kernel(
+__global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 	const UpsweepArgs a) {
 
 	__shared__ unsigned sHist[kMaxBins];
@@ -78,38 +78,60 @@ __global__ void __launch_bounds__(kUpThreads) upsweep_kernel(
 	for(int i = tid; i < totalBins; i += kUpThreads) sHist[i] = 0;
 	__syncthreads();
 
-	for(long long c = blockIdx.x; c * kUpChunk < a.n; c += gridDim.x) {
-		const long long base = c * kUpChunk;
-		unsigned k[kUpKeysPerThread];
-		int nValid;
-		if(a.vecOk && base + kUpChunk <= a.n) {
-			const uint4* src = reinterpret_cast<const uint4*>(a.keys + base);
-#pragma unroll
-			for(int i = 0; i < kUpKeysPerThread / 4; ++i) {
-				uint4 q = ld_stream_u4(src + i * kUpThreads + tid);
-				k[4 * i + 0] = q.x;
-				k[4 * i + 1] = q.y;
-				k[4 * i + 2] = q.z;
-				k[4 * i + 3] = q.w;
-			}
-			nValid = kUpKeysPerThread;
-		} else {
-			// Element (i, j) of this thread sits at base + (i*NT + tid)*4 + j,
-			// increasing in (i, j): the valid elements form a prefix.
-			nValid = 0;
-#pragma unroll
-			for(int i = 0; i < kUpKeysPerThread / 4; ++i)
-#pragma unroll
-				for(int j = 0; j < 4; ++j) {
-					long long idx = base + (long long)(i * kUpThreads + tid) * 4 + j;
-					bool valid = idx < a.n;
-					k[4 * i + j] = valid ? a.keys[idx] : 0u;
-					nValid += valid;
-				}
-		}
+	auto count_all = [&](const unsigned (&k)[kUpKeysPerThread], int nValid) {
 		for(int p = 0; p < numPasses; ++p)
 			count_digits(sHist + a.plan.binBase[p], k, nValid, a.plan.shift[p],
 				(1u << a.plan.width[p]) - 1);
+	};
+
+	// Full chunks with 16-byte loads, the next chunk's loads in flight while
+	// the current one is counted.
+	const long long fullChunks = a.vecOk ? a.n / kUpChunk : 0;
+	long long c = blockIdx.x;
+	uint4 next[kUpKeysPerThread / 4];
+	if(c < fullChunks) {
+		const uint4* src = reinterpret_cast<const uint4*>(a.keys + c * kUpChunk);
+#pragma unroll
+		for(int i = 0; i < kUpKeysPerThread / 4; ++i)
+			next[i] = ld_stream_u4(src + i * kUpThreads + tid);
+	}
+	for(; c < fullChunks; c += gridDim.x) {
+		unsigned k[kUpKeysPerThread];
+#pragma unroll
+		for(int i = 0; i < kUpKeysPerThread / 4; ++i) {
+			k[4 * i + 0] = next[i].x;
+			k[4 * i + 1] = next[i].y;
+			k[4 * i + 2] = next[i].z;
+			k[4 * i + 3] = next[i].w;
+		}
+		if(c + gridDim.x < fullChunks) {
+			const uint4* src = reinterpret_cast<const uint4*>(
+				a.keys + (c + gridDim.x) * kUpChunk);
+#pragma unroll
+			for(int i = 0; i < kUpKeysPerThread / 4; ++i)
+				next[i] = ld_stream_u4(src + i * kUpThreads + tid);
+		}
+		count_all(k, kUpKeysPerThread);
+	}
+
+	// The rest (a ragged tail, or everything when the keys are not 16-byte
+	// aligned) with plain loads. Element (i, j) of this thread sits at
+	// base + (i*NT + tid)*4 + j, increasing in (i, j): the valid elements
+	// form a prefix.
+	for(long long r = fullChunks + blockIdx.x; r * kUpChunk < a.n; r += gridDim.x) {
+		const long long base = r * kUpChunk;
+		unsigned k[kUpKeysPerThread];
+		int nValid = 0;
+#pragma unroll
+		for(int i = 0; i < kUpKeysPerThread / 4; ++i)
+#pragma unroll
+			for(int j = 0; j < 4; ++j) {
+				long long idx = base + (long long)(i * kUpThreads + tid) * 4 + j;
+				bool valid = idx < a.n;
+				k[4 * i + j] = valid ? a.keys[idx] : 0u;
+				nValid += valid;
+			}
+		count_all(k, nValid);
 	}
 	__syncthreads();
 
@@ -177,6 +199,7 @@ constexpr unsigned long long kFlagInclusive = 2ull << 32;
 template<int VM> struct PassConfig {
 	static constexpr int kThreads = 256;
 	static constexpr int kItems = 16;
+	static constexpr int kMinBlocks = 4;
 };
 
 template<int VM> struct PassLayout {
@@ -184,7 +207,9 @@ template<int VM> struct PassLayout {
 	static constexpr int IPT = PassConfig<VM>::kItems;
 	static constexpr int TILE = NT * IPT;
 	static constexpr int NW = NT / 32;
-	static constexpr int NSTAGE = VM >= 2 ? 2 : (VM == 1 ? 1 : 0);
+	// Value staging buffers: index mode writes its generated indices into
+	// one, value arrays are double-buffered.
+	static constexpr int NSTAGE = VM >= 2 ? 2 : (VM == 0 ? 0 : 1);
 	// Word offsets into dynamic shared memory.
 	static constexpr int kKeys = 0;
 	static constexpr int kVals = kKeys + TILE;
@@ -215,9 +240,64 @@ __device__ __forceinline__ void copy_tile(const PassArgs& a, long long start,
 	}
 }
 
+// Lanes of the warp whose 8-bit digit equals this lane's, from one ballot per
+// digit bit (a lane keeps the ballot where its bit is set, the complement
+// where it is clear).
+__device__ __forceinline__ unsigned match_digit8(unsigned d) {
+	unsigned peers = 0xffffffffu;
+#pragma unroll
+	for(int b = 0; b < 8; ++b) {
+		const bool set = (d >> b) & 1u;
+		const unsigned bal = __ballot_sync(0xffffffffu, set);
+		peers &= set ? bal : ~bal;
+	}
+	return peers;
+}
+
+// Decoupled lookback of one digit: sum the counts of the tiles before `tile`
+// back to the nearest one that published an inclusive prefix. Reads up to
+// four predecessors per step so that a walk over published aggregates costs
+// one memory round trip per four tiles.
+__device__ __forceinline__ unsigned lookback_digit(
+	const unsigned long long* status, int tile, int digit, unsigned epoch,
+	bool* timedOut) {
+	unsigned excl = 0;
+	int j = tile - 1;
+	WaitBudget budget;
+	while(true) {
+		unsigned long long w[4];
+#pragma unroll
+		for(int k = 0; k < 4; ++k)
+			w[k] = j - k >= 0
+				? ld_relaxed_u64(status + (size_t)(j - k) * kDigitBins + digit) : 0ull;
+		int consumed = 0;
+		bool done = false, stalled = false;
+#pragma unroll
+		for(int k = 0; k < 4; ++k) {
+			if(done || stalled) continue;
+			const unsigned long long flag = w[k] & (3ull << 32);
+			if(j - k < 0 || (w[k] >> 34) != epoch || !flag) {
+				stalled = true;
+				continue;
+			}
+			excl += (unsigned)w[k];
+			++consumed;
+			if(flag == kFlagInclusive) done = true;
+		}
+		if(done) break;
+		j -= consumed;
+		if(consumed) budget = WaitBudget();
+		else if(!budget.poll()) {
+			*timedOut = true;
+			break;
+		}
+	}
+	return excl;
+}
+
 template<int VM>
-__global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
-	const PassArgs a) {
+__global__ void __launch_bounds__(PassLayout<VM>::NT, PassConfig<VM>::kMinBlocks)
+onesweep_kernel(const PassArgs a) {
 
 	using L = PassLayout<VM>;
 	constexpr int NT = L::NT;
@@ -225,6 +305,9 @@ __global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
 	constexpr int TILE = L::TILE;
 	constexpr int NW = L::NW;
 	constexpr int NV = VM > 0 ? VM : 0;
+	// Value arrays (or generated indices) reordered in shared memory before
+	// the lookback; the rest stream through the staging buffers after it.
+	constexpr int NPRE = VM == kValueIndex ? 1 : (NV < 2 ? NV : 2);
 
 	extern __shared__ __align__(128) unsigned smem[];
 	unsigned* sKeys = smem + L::kKeys;
@@ -247,13 +330,10 @@ __global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
 		if(t == (unsigned)a.numTiles - 1) *a.tileCounter = 0;
 		sTile[0] = t;
 		sTile[1] = *a.trivial;
-		if(NV > 0 && a.useBulk) {
+		if(a.useBulk) {
 			mbar_init(&sBar[0], 1);
 			mbar_init(&sBar[1], 1);
 			mbar_init(&sBar[2], 1);
-			fence_mbar_init();
-		} else if(a.useBulk) {
-			mbar_init(&sBar[0], 1);
 			fence_mbar_init();
 		}
 	}
@@ -303,30 +383,30 @@ __global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
 
 	const unsigned mask = (1u << a.width) - 1;
 	const int shift = a.shift;
+	// Padding of a partial tile gets digit 255: it ranks after every real
+	// key (it is last in input order and 255 is the last bin) and is never
+	// stored.
 	auto digit_of = [&](int i) -> unsigned {
 		int idx = warpBase + i * 32 + lane;
 		return idx < count ? (keys[i] >> shift) & mask : (kDigitBins - 1);
 	};
 
 	// Stable rank within the warp: peers with the same digit are ranked by
-	// lane, items in order, each warp keeping a running count per digit.
+	// lane, items in order. The highest peer adds the group to the warp's
+	// running count of the digit; the atomic's old value, broadcast, is the
+	// group's base. The shuffle orders each item's update before the next.
 	unsigned* myHist = sWarpHist + warp * kDigitBins;
 	const unsigned ltMask = lanemask_lt();
 	unsigned rank[IPT];
 #pragma unroll
 	for(int i = 0; i < IPT; ++i) {
-		unsigned d = digit_of(i);
-		unsigned peers = __match_any_sync(0xffffffffu, d);
-		int leader = 31 - __clz(peers);
-		unsigned before = __popc(peers & ltMask);
+		const unsigned d = digit_of(i);
+		const unsigned peers = match_digit8(d);
+		const int leader = 31 - __clz(peers);
 		unsigned base = 0;
-		if(lane == leader) {
-			base = myHist[d];
-			myHist[d] = base + __popc(peers);
-		}
+		if(lane == leader) base = atomicAdd(&myHist[d], (unsigned)__popc(peers));
 		base = __shfl_sync(0xffffffffu, base, leader);
-		rank[i] = base + before;
-		__syncwarp();
+		rank[i] = base + __popc(peers & ltMask);
 	}
 	__syncthreads();
 
@@ -340,100 +420,50 @@ __global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
 			total += c;
 		}
 	}
-	unsigned incl = warp_inclusive_scan(total, lane);
+	const unsigned incl = warp_inclusive_scan(total, lane);
 	if(lane == 31 && tid < kDigitBins) sScan[warp] = incl;
 	__syncthreads();
 
+	// Publish this tile's digit counts as soon as they are known.
+	const unsigned long long epochBits = (unsigned long long)a.epoch << 34;
+	unsigned digStart = 0;
+	unsigned mine = 0;
 	if(tid < kDigitBins) {
 		unsigned prefix = 0;
 		for(int w = 0; w < warp; ++w) prefix += sScan[w];
-		const unsigned digStart = prefix + incl - total;
+		digStart = prefix + incl - total;
 		sDigStart[tid] = digStart;
-
-		if(tid <= (int)mask) {
-			// Padding of a partial tile sits in digit 255 only, past every
-			// real key of that digit; it is not published.
-			unsigned mine = total;
-			if(tid == kDigitBins - 1) mine -= TILE - count;
-			const unsigned long long epoch = (unsigned long long)a.epoch << 34;
+		mine = total;
+		if(tid == kDigitBins - 1) mine -= TILE - count;
+		if(tid <= (int)mask && tile != a.failTile) {
 			unsigned long long* st = a.status + (size_t)tile * kDigitBins + tid;
-			unsigned excl = 0;
-			if(tile == a.failTile) {
-				// Injected fault (tests only): this tile never publishes, so
-				// the tiles after it run their bounded waits out.
-				if(tid == 0) report_error(a.devError, a.hostError, kErrInjected);
-			} else if(tile == 0) {
-				st_relaxed_u64(st, epoch | kFlagInclusive | mine);
-			} else {
-				st_relaxed_u64(st, epoch | kFlagAggregate | mine);
-				const unsigned long long* look = st - kDigitBins;
-				WaitBudget budget;
-				while(true) {
-					unsigned long long w = ld_relaxed_u64(look);
-					unsigned long long flag = w & (3ull << 32);
-					if((w >> 34) != a.epoch || !flag) {
-						if(!budget.poll()) {
-							report_error(a.devError, a.hostError, kErrLookbackTimeout);
-							break;
-						}
-						continue;
-					}
-					excl += (unsigned)w;
-					if(flag == kFlagInclusive) break;
-					look -= kDigitBins;
-					budget = WaitBudget();
-				}
-				st_relaxed_u64(st, epoch | kFlagInclusive | (excl + mine));
-			}
-			sScatter[tid] = (int)(a.digitOffsets[tid] + excl - digStart);
+			st_relaxed_u64(st, epochBits | (tile == 0 ? kFlagInclusive : kFlagAggregate)
+				| mine);
 		}
 	}
 	__syncthreads();
 
-	// Reorder the tile in shared memory into digit runs.
+	// Reorder the tile in shared memory into digit runs: keys, then the
+	// value arrays whose tiles are already staged (or generated indices).
 #pragma unroll
 	for(int i = 0; i < IPT; ++i) {
-		unsigned d = digit_of(i);
+		const unsigned d = digit_of(i);
 		rank[i] += sDigStart[d] + sWarpHist[warp * kDigitBins + d];
 		sKeys[rank[i]] = keys[i];
 	}
-	__syncthreads();
-
-	// Write each run to its global position: element p of the reordered tile
-	// goes to scatter[digit] + p, consecutive p -> consecutive addresses.
-	int dst[IPT];
-#pragma unroll
-	for(int j = 0; j < IPT; ++j) {
-		int p = j * NT + tid;
-		dst[j] = -1;
-		if(p < count) {
-			unsigned k = sKeys[p];
-			dst[j] = sScatter[(k >> shift) & mask] + p;
-			a.buf.keysOut[dst[j]] = k;
-		}
-	}
-
 	if constexpr(VM == kValueIndex) {
-		__syncthreads();
 #pragma unroll
 		for(int i = 0; i < IPT; ++i)
-			sKeys[rank[i]] = (unsigned)(tileStart + warpBase + i * 32 + lane);
-		__syncthreads();
-#pragma unroll
-		for(int j = 0; j < IPT; ++j)
-			if(dst[j] >= 0) a.buf.valsOut[0][dst[j]] = sKeys[j * NT + tid];
+			sVals[rank[i]] = (unsigned)(tileStart + warpBase + i * 32 + lane);
 	}
-
 #pragma unroll
-	for(int v = 0; v < NV; ++v) {
+	for(int v = 0; v < (VM > 0 ? NPRE : 0); ++v) {
 		unsigned vals[IPT];
 		if(bulk) {
-			const int stage = v & 1;
-			if(!mbar_wait_bounded(&sBar[1 + stage], (v >> 1) & 1))
+			if(!mbar_wait_bounded(&sBar[1 + v], 0))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 #pragma unroll
-			for(int i = 0; i < IPT; ++i)
-				vals[i] = sVals[stage * TILE + warpBase + i * 32 + lane];
+			for(int i = 0; i < IPT; ++i) vals[i] = sVals[v * TILE + warpBase + i * 32 + lane];
 		} else {
 #pragma unroll
 			for(int i = 0; i < IPT; ++i) {
@@ -441,21 +471,84 @@ __global__ void __launch_bounds__(PassLayout<VM>::NT) onesweep_kernel(
 				vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
 			}
 		}
-		// Everyone is done with the staging buffer and with sKeys.
 		__syncthreads();
-		if(bulk && tid == 0 && v + 2 < NV) {
-			const int stage = v & 1;
+#pragma unroll
+		for(int i = 0; i < IPT; ++i) sVals[v * TILE + rank[i]] = vals[i];
+	}
+
+	// Global offsets: the digit's start over the whole array plus the counts
+	// of the tiles before this one.
+	if(tid <= (int)mask) {
+		unsigned excl = 0;
+		if(tile == a.failTile) {
+			// Injected fault (tests only): this tile never publishes, so the
+			// tiles after it run their bounded waits out.
+			if(tid == 0) report_error(a.devError, a.hostError, kErrInjected);
+		} else if(tile > 0) {
+			bool timedOut = false;
+			excl = lookback_digit(a.status, tile, tid, a.epoch, &timedOut);
+			if(timedOut) report_error(a.devError, a.hostError, kErrLookbackTimeout);
+			st_relaxed_u64(a.status + (size_t)tile * kDigitBins + tid,
+				epochBits | kFlagInclusive | (excl + mine));
+		}
+		sScatter[tid] = (int)(a.digitOffsets[tid] + excl - digStart);
+	}
+	__syncthreads();
+
+	// Write each run to its global position: element p of the reordered tile
+	// goes to scatter[digit] + p, consecutive p -> consecutive addresses.
+#pragma unroll
+	for(int j = 0; j < IPT; ++j) {
+		const int p = j * NT + tid;
+		if(p < count) {
+			const unsigned k = sKeys[p];
+			const int dst = sScatter[(k >> shift) & mask] + p;
+			a.buf.keysOut[dst] = k;
+			if constexpr(VM == kValueIndex) a.buf.valsOut[0][dst] = sVals[p];
+#pragma unroll
+			for(int v = 0; v < (VM > 0 ? NPRE : 0); ++v)
+				a.buf.valsOut[v][dst] = sVals[v * TILE + p];
+		}
+	}
+
+	// Remaining value arrays stream through the two staging buffers.
+#pragma unroll
+	for(int v = NPRE; v < NV; ++v) {
+		const int stage = v & 1;
+		unsigned* buf = sVals + stage * TILE;
+		// Everyone is done with this staging buffer (its last reader was the
+		// store of array v - 2): refill it.
+		__syncthreads();
+		if(bulk && tid == 0) {
 			fence_proxy_async_smem();
 			mbar_arrive_expect_tx(&sBar[1 + stage], TILE * 4);
-			bulk_load(sVals + stage * TILE, a.buf.valsIn[v + 2] + tileStart,
-				TILE * 4, &sBar[1 + stage]);
+			bulk_load(buf, a.buf.valsIn[v] + tileStart, TILE * 4, &sBar[1 + stage]);
 		}
+		unsigned vals[IPT];
+		if(bulk) {
+			if(!mbar_wait_bounded(&sBar[1 + stage], (v >> 1) & 1))
+				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 #pragma unroll
-		for(int i = 0; i < IPT; ++i) sKeys[rank[i]] = vals[i];
+			for(int i = 0; i < IPT; ++i) vals[i] = buf[warpBase + i * 32 + lane];
+		} else {
+#pragma unroll
+			for(int i = 0; i < IPT; ++i) {
+				int idx = warpBase + i * 32 + lane;
+				vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
+			}
+		}
 		__syncthreads();
 #pragma unroll
-		for(int j = 0; j < IPT; ++j)
-			if(dst[j] >= 0) a.buf.valsOut[v][dst[j]] = sKeys[j * NT + tid];
+		for(int i = 0; i < IPT; ++i) buf[rank[i]] = vals[i];
+		__syncthreads();
+#pragma unroll
+		for(int j = 0; j < IPT; ++j) {
+			const int p = j * NT + tid;
+			if(p < count) {
+				const int dst = sScatter[(sKeys[p] >> shift) & mask] + p;
+				a.buf.valsOut[v][dst] = buf[p];
+			}
+		}
 	}
 }
 
@@ -519,7 +612,7 @@ cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
 	a.ctrl = ctrl;
 	a.hostError = hostError;
 	long long chunks = ((long long)n + kUpChunk - 1) / kUpChunk;
-	int grid = (int)std::min<long long>(chunks, (long long)numSMs * 2);
+	int grid = (int)std::min<long long>(chunks, (long long)numSMs * 3);
 	if(grid < 1) grid = 1;
 	upsweep_kernel<<<grid, kUpThreads, 0, stream>>>(a);
 	return cudaGetLastError();

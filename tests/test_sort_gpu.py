@@ -238,17 +238,14 @@ def test_library_managed_data(engine, lib, oracle_mod):
     sd = api.MgpuSortData()
     sd.attach_key(kp)
     assert sd.alloc(engine, n, -1) == 0
+    sd.firstBit, sd.endBit = 0, 32          # Alloc leaves the bit range to the caller
     assert sd.keys[0] == kp and sd.keys[1] and sd.values[0][0] and sd.values[0][1]
     torch.cuda.synchronize()
     assert engine.sort_array(sd) == 0
     assert engine.synchronize() == 0
     ek, (ev,) = expect(oracle_mod, keys, [], -1, 0, 32)
-    out = np.empty(n, np.uint32)
-    import ctypes as C
-    # read through torch: wrap the result pointer
-    res = kt if sd.keys[0] == kp else None
-    if res is not None:
-        assert np.array_equal(kt.cpu().numpy().view(np.uint32), ek)
+    assert sd.parity == 0 and sd.keys[0] == kp     # four passes: back in place
+    assert np.array_equal(kt.cpu().numpy().view(np.uint32), ek)
     sd.reset()                       # frees only the library's buffers
     assert sd.keys[0] == 0 and sd.keys[1] == 0
     torch.cuda.synchronize()
