@@ -47,6 +47,38 @@ sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable);
 sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches);
 
+/* Largest numElements that sortArrayNoAlloc accepts (4 Mi elements). */
+#define SORT_NOALLOC_MAX_ELEMENTS 4194304
+
+/* sortArray for callers that cannot allocate device memory. No counterpart
+ * in the reference.
+ *
+ * Who needs it: programs that give all of a GPU's memory to their own
+ * allocator or budget up front (so any allocation by a library fails or
+ * breaks the budget), and latency-critical loops in which a cudaMalloc or
+ * cudaFree would synchronize the device and stall other streams. sortArray's
+ * engine allocates its scratch; this entry point takes no engine and calls no
+ * cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Its scratch is one file-scope device array of about 2 MiB (a control block
+ * plus lookback status for SORT_NOALLOC_MAX_ELEMENTS elements), held by every
+ * GPU that loads the library until the process exits. The first call on a
+ * device, with that device current, looks up the array's device address and
+ * clears it (a synchronous cudaMemset); make that first call before any
+ * stream capture.
+ *
+ * Semantics are sortArray's (same buffers, swaps, parity, bit range, value
+ * modes, results), on `stream`, except that earlyExit is ignored (every pass
+ * runs; the result is the same) and the call returns only after the sort has
+ * finished, with SORT_STATUS_KERNEL_ERROR if a device-side wait ran out.
+ * numElements above SORT_NOALLOC_MAX_ELEMENTS returns
+ * SORT_STATUS_CONFIG_NOT_SUPPORTED without device work.
+ *
+ * Every call shares the one array: calls whose work overlaps on the GPU (from
+ * several host threads, or on several streams) race and corrupt each other's
+ * results; issue them one after another. */
+sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t data, CUstream stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

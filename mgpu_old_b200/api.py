@@ -65,8 +65,11 @@ EXPORTED_SYMBOLS = (
     "sortFreeData", "sortArray", "sortArrayEx", "sortHost", "sortDevice",
     # mgpusort_b200.h (no reference counterpart)
     "sortArrayAsync", "sortSynchronize", "sortPlanPasses", "sortInjectFault",
-    "sortEnableKernelTiming", "sortReadKernelTiming",
+    "sortEnableKernelTiming", "sortReadKernelTiming", "sortArrayNoAlloc",
 )
+
+# Largest numElements accepted by sortArrayNoAlloc (SORT_NOALLOC_MAX_ELEMENTS).
+NOALLOC_MAX_ELEMENTS = 4194304
 
 _lib = None
 
@@ -103,6 +106,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "sortEnableKernelTiming": (c_int, [engine_t, c_int]),
         "sortReadKernelTiming": (c_int, [engine_t, POINTER(ctypes.c_double), POINTER(c_int),
                                          POINTER(ctypes.c_double), POINTER(c_int)]),
+        "sortArrayNoAlloc": (c_int, [data_t, c_void_p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -210,6 +214,12 @@ class MgpuSort:
             assert values.dtype == np.uint32 and values.flags.c_contiguous
             vp = values.ctypes.data_as(POINTER(c_uint))
         return load_library().sortHost(self._engine, kp, vp, int(keys.size), num_bits)
+
+
+def sort_array_no_alloc(data: SortData, stream: int = 0) -> int:
+    """sortArrayNoAlloc: sortArray without an engine and without allocating;
+    waits for the sort. For callers whose device memory is all pre-budgeted."""
+    return load_library().sortArrayNoAlloc(ctypes.byref(data), c_void_p(stream))
 
 
 class MgpuSortData(SortData):
