@@ -32,17 +32,20 @@ int SORTAPI sortPlanPasses(int firstBit, int endBit, int bitPass,
 	int* widths);
 
 /* Fault injection for tests of the device-side bounded waits: in the next
- * pass launched by this engine, tile `tile` skips publishing its digit counts,
- * so every later tile's lookback wait runs out (about half a second) and the
- * sort reports SORT_STATUS_KERNEL_ERROR through sortSynchronize. -1 turns it
- * off. Nothing faults or traps; the engine is usable afterwards. */
+ * pass launched by this engine, the CTA that sorts tile `tile` (4096
+ * elements each) also waits on a barrier that nothing completes, so that
+ * bounded wait runs out (about half a second) and the sort reports
+ * SORT_STATUS_KERNEL_ERROR through sortSynchronize. -1 turns it off. Nothing
+ * faults, traps or hangs; the engine is usable afterwards. */
 sortStatus_t SORTAPI sortInjectFault(sortEngine_t engine, int tile);
 
-/* Kernel timing for benchmarks: while enabled, every kernel launch of the
- * engine is bracketed by CUDA events on its stream. sortReadKernelTiming
- * waits for them, returns the summed milliseconds and launch counts of the
- * upsweep (histogram) kernel and of the onesweep pass kernel since the last
- * read, and starts a new count. Any argument may be NULL. */
+/* Kernel timing for benchmarks: while enabled, the engine brackets its
+ * launches with CUDA events on its stream. sortReadKernelTiming waits for
+ * them and returns, since the last read, the summed milliseconds and counts
+ * of the counting launches (each pass's count + scan kernels, and the
+ * earlyExit histogram kernel) as "upsweep", and of the sort kernel launches
+ * (one per pass) as "pass"; then it starts a new count. Any argument may be
+ * NULL. */
 sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable);
 sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches);
@@ -61,8 +64,8 @@ sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
  * cudaMalloc, cudaFree or other allocating routine.
  *
  * Its scratch is one file-scope device array of about 2 MiB (a control block
- * plus lookback status for SORT_NOALLOC_MAX_ELEMENTS elements), held by every
- * GPU that loads the library until the process exits. The first call on a
+ * plus the per-pass range counts and offsets), held by every GPU that loads
+ * the library until the process exits. The first call on a
  * device, with that device current, looks up the array's device address and
  * clears it (a synchronous cudaMemset); make that first call before any
  * stream capture.

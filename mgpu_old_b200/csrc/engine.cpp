@@ -63,9 +63,6 @@ const char* const kStatusNames[] = {
 // (mgpusort.cpp:663, 696).
 constexpr int kAllocRound = 2048;
 
-// Lookback epochs are 30 bits wide.
-constexpr unsigned kMaxEpoch = (1u << 30) - 1;
-
 int round_up(int x, int m) { return (int)(((long long)x + m - 1) / m * m); }
 
 } // namespace
@@ -75,9 +72,8 @@ struct sortEngine_d {
 	int device = 0;
 	int numSMs = 0;
 	mgpusort::Control* ctrl = nullptr;
-	unsigned long long* status = nullptr;
-	size_t statusBytes = 0;
-	unsigned epoch = 0;
+	// Per-pass scratch: range digit counts, their prefixes, digit totals.
+	unsigned* scratch = nullptr;
 	// Host-mapped error word written by kernels, read without synchronizing.
 	volatile unsigned* hostError = nullptr;
 	unsigned* hostErrorDev = nullptr;
@@ -128,7 +124,7 @@ void destroy_engine(sortEngine_d* e) {
 		cudaEventDestroy(t.stop);
 	}
 	if(e->ctrl) cudaFree(e->ctrl);
-	if(e->status) cudaFree(e->status);
+	if(e->scratch) cudaFree(e->scratch);
 	if(e->hostError) cudaFreeHost(const_cast<unsigned*>(e->hostError));
 	if(e->hostTrivial) cudaFreeHost(e->hostTrivial);
 	if(e->done) cudaEventDestroy(e->done);
@@ -191,36 +187,6 @@ sortStatus_t take_device_error(sortEngine_d* e) {
 	return SORT_STATUS_KERNEL_ERROR;
 }
 
-sortStatus_t ensure_status(sortEngine_d* e, size_t bytes) {
-	if(bytes <= e->statusBytes) return SORT_STATUS_SUCCESS;
-	// Grow only (like the reference's scratch, mgpusort.cpp:319-343). The
-	// old buffer may still be read by queued work: cudaFree waits for it.
-	if(e->status) cudaFree(e->status);
-	e->status = nullptr;
-	e->statusBytes = 0;
-	void* p = nullptr;
-	if(cudaMalloc(&p, bytes) != cudaSuccess) {
-		cudaGetLastError();
-		return SORT_STATUS_DEVICE_ALLOC_FAILED;
-	}
-	// Fresh memory may hold any bits; epoch 0 is never used by a pass.
-	if(cudaMemset(p, 0, bytes) != cudaSuccess) {
-		cudaFree(p);
-		return SORT_STATUS_DEVICE_ERROR;
-	}
-	e->status = static_cast<unsigned long long*>(p);
-	e->statusBytes = bytes;
-	return SORT_STATUS_SUCCESS;
-}
-
-unsigned next_epoch(sortEngine_d* e, cudaStream_t stream) {
-	if(e->epoch >= kMaxEpoch) {
-		cudaMemsetAsync(e->status, 0, e->statusBytes, stream);
-		e->epoch = 0;
-	}
-	return ++e->epoch;
-}
-
 void swap_buffers(sortData_d* d) {
 	std::swap(d->keys[0], d->keys[1]);
 	for(int i = 0; i < 6; ++i) std::swap(d->values[i][0], d->values[i][1]);
@@ -255,13 +221,6 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 	if(!make_plan(d->firstBit, numBits, bitPass, &plan))
 		return SORT_STATUS_INTERNAL_ERROR;
 
-	size_t statusBytes = mgpusort::pass_status_bytes(n, numArrays);
-	if(indexMode)
-		statusBytes = std::max(statusBytes,
-			mgpusort::pass_status_bytes(n, mgpusort::kValueIndex));
-	sortStatus_t st = ensure_status(e, statusBytes);
-	if(st != SORT_STATUS_SUCCESS) return st;
-
 	if(e->dirty) {
 		if(cudaMemsetAsync(e->ctrl, 0, sizeof(mgpusort::Control), stream)
 			!= cudaSuccess) return SORT_STATUS_DEVICE_ERROR;
@@ -273,18 +232,21 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 	for(int i = 0; i < numArrays; ++i)
 		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
 
-	int slot = timing_begin(e, kTimedUpsweep, stream);
-	cudaError_t ce = mgpusort::launch_upsweep(
-		reinterpret_cast<const unsigned*>(d->keys[0]), n, plan, e->ctrl,
-		e->hostErrorDev, e->numSMs, stream);
-	timing_end(e, slot, stream);
-	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-
-	// earlyExit: one read-back of the per-pass "single digit" flags, then
-	// skip those passes (the reference reads its detect counters back per
-	// pass for the same purpose, mgpusort.cpp:434-451).
+	// earlyExit: one upsweep builds every pass's digit histogram, one
+	// read-back of the per-pass "single digit" flags, then those passes are
+	// skipped (the reference reads its detect counters back per pass for the
+	// same purpose, mgpusort.cpp:434-451). Without earlyExit a single-digit
+	// pass runs as a straight copy.
 	bool skip[mgpusort::kMaxPasses] = {};
+	int slot = -1;
+	cudaError_t ce = cudaSuccess;
 	if(d->earlyExit) {
+		slot = timing_begin(e, kTimedUpsweep, stream);
+		ce = mgpusort::launch_upsweep(
+			reinterpret_cast<const unsigned*>(d->keys[0]), n, plan, e->ctrl,
+			e->hostErrorDev, e->numSMs, stream);
+		timing_end(e, slot, stream);
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
 		if(cudaMemcpyAsync(e->hostTrivial, e->ctrl->trivial,
 			sizeof(unsigned) * plan.numPasses, cudaMemcpyDeviceToHost, stream)
 			!= cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
@@ -306,10 +268,14 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
 			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
 		}
-		const unsigned epoch = next_epoch(e, stream);
+		slot = timing_begin(e, kTimedUpsweep, stream);
+		ce = mgpusort::launch_pass_count(buf, vm, n, p, plan, e->scratch, e->numSMs,
+			stream);
+		timing_end(e, slot, stream);
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
 		slot = timing_begin(e, kTimedPass, stream);
-		ce = mgpusort::launch_pass(buf, vm, n, p, plan, e->ctrl, e->status,
-			epoch, bulk, e->failTile, e->hostErrorDev, stream);
+		ce = mgpusort::launch_pass_sort(buf, vm, n, p, plan, e->ctrl, e->scratch,
+			bulk, e->failTile, e->hostErrorDev, e->numSMs, stream);
 		timing_end(e, slot, stream);
 		e->failTile = -1;
 		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
@@ -367,6 +333,9 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 		e->ctrl = static_cast<mgpusort::Control*>(p);
 		if(cudaMemset(e->ctrl, 0, sizeof(mgpusort::Control)) != cudaSuccess)
 			status = SORT_STATUS_DEVICE_ERROR;
+		else if(cudaMalloc(&p, mgpusort::pass_scratch_bytes()) != cudaSuccess)
+			status = SORT_STATUS_DEVICE_ALLOC_FAILED;
+		else e->scratch = static_cast<unsigned*>(p);
 	}
 	if(status == SORT_STATUS_SUCCESS) {
 		void* h = nullptr;

@@ -6,13 +6,14 @@
 // fails any allocation outside it), and latency-critical loops where a
 // cudaMalloc or cudaFree would synchronize the device and stall every other
 // stream. sortArray cannot serve them, because its engine allocates its
-// scratch (control block, lookback status, a mapped error word).
+// scratch (control block, per-pass range counts, a mapped error word).
 //
 // This entry point needs no engine and allocates nothing. Its scratch is the
-// file-scope array below: a control block plus lookback status for up to
-// SORT_NOALLOC_MAX_ELEMENTS elements, about 2 MiB, which each GPU that loads
-// this module holds until the process exits. The caller passes the key and
-// value buffers in a sortData_d, exactly as for sortArray.
+// file-scope array below: a control block plus the per-pass range counts and
+// offsets, about 2 MiB, which each GPU that loads this module holds until the
+// process exits. It accepts up to SORT_NOALLOC_MAX_ELEMENTS elements. The
+// caller passes the key and value buffers in a sortData_d, exactly as for
+// sortArray.
 
 // The library is built with hidden visibility; the C ABI is all it exports.
 #pragma GCC visibility push(default)
@@ -29,24 +30,20 @@
 
 namespace {
 
-// The status area is sized for pass tiles of at least this many elements;
-// a call whose plan would need more status than that is rejected.
-constexpr size_t kSizedTile = 4096;
-constexpr size_t kStatusWords = (size_t)SORT_NOALLOC_MAX_ELEMENTS / kSizedTile
-	* mgpusort::kDigitBins;
 constexpr size_t kControlWords =
 	(sizeof(mgpusort::Control) + 255) / 256 * 256 / sizeof(unsigned long long);
-constexpr size_t kScratchWords = kControlWords + kStatusWords;
+constexpr size_t kPassWords =
+	(mgpusort::kPassScratchWords * sizeof(unsigned) + 7) / sizeof(unsigned long long);
+constexpr size_t kScratchWords = kControlWords + kPassWords;
 
 } // namespace
 
-// The scratch: [Control, padded to 256 bytes][lookback status words].
+// The scratch: [Control, padded to 256 bytes][pass scratch].
 static __device__ __align__(256) unsigned long long g_noAllocScratch[kScratchWords];
 
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr unsigned kMaxEpoch = (1u << 30) - 1;
 
 // Host-side view of one device's scratch. `scratch` is the device address of
 // g_noAllocScratch on that device: in host code the array's own name is only
@@ -55,7 +52,6 @@ struct DeviceScratch {
 	bool ready;
 	unsigned long long* scratch;
 	int numSMs;
-	unsigned epoch;
 };
 
 DeviceScratch g_devices[kMaxDevices];
@@ -92,7 +88,6 @@ sortStatus_t set_up(int device, DeviceScratch* s) {
 	}
 	s->scratch = static_cast<unsigned long long*>(p);
 	s->numSMs = sms;
-	s->epoch = 0;
 	s->ready = true;
 	return SORT_STATUS_SUCCESS;
 }
@@ -122,11 +117,6 @@ extern "C" sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t d, CUstream cuStream
 		if(!d->values[i][0] || !d->values[i][1]) return SORT_STATUS_INVALID_VALUE;
 	if(n > SORT_NOALLOC_MAX_ELEMENTS) return SORT_STATUS_CONFIG_NOT_SUPPORTED;
 	if(!n) return SORT_STATUS_SUCCESS;
-	const size_t statusBytes = kStatusWords * sizeof(unsigned long long);
-	if(mgpusort::pass_status_bytes(n, numArrays) > statusBytes ||
-		(indexMode && mgpusort::pass_status_bytes(n, mgpusort::kValueIndex)
-			> statusBytes))
-		return SORT_STATUS_CONFIG_NOT_SUPPORTED;
 
 	// The same plan as sortArray.
 	int widths[mgpusort::kMaxPasses];
@@ -156,11 +146,12 @@ extern "C" sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t d, CUstream cuStream
 		if(st != SORT_STATUS_SUCCESS) return st;
 	}
 	mgpusort::Control* ctrl = reinterpret_cast<mgpusort::Control*>(s.scratch);
-	unsigned long long* status = s.scratch + kControlWords;
+	unsigned* passScratch = reinterpret_cast<unsigned*>(s.scratch + kControlWords);
 	cudaStream_t stream = reinterpret_cast<cudaStream_t>(cuStream);
 
-	// The array keeps the previous call's contents. The control block must
-	// start at zero; lookback words are told apart by their epoch.
+	// The array keeps the previous call's contents. The control block (its
+	// error word) must start at zero; every pass rewrites the pass scratch
+	// before reading it.
 	if(cudaMemsetAsync(ctrl, 0, sizeof(mgpusort::Control), stream) != cudaSuccess) {
 		cudaGetLastError();
 		return SORT_STATUS_DEVICE_ERROR;
@@ -170,10 +161,7 @@ extern "C" sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t d, CUstream cuStream
 	for(int i = 0; i < numArrays; ++i)
 		for(int j = 0; j < 2; ++j) bulk = bulk && (d->values[i][j] & 15) == 0;
 
-	cudaError_t ce = mgpusort::launch_upsweep(
-		reinterpret_cast<const unsigned*>(d->keys[0]), n, plan, ctrl, nullptr,
-		s.numSMs, stream);
-	if(ce != cudaSuccess) return SORT_STATUS_LAUNCH_ERROR;
+	cudaError_t ce = cudaSuccess;
 	for(int p = 0; p < passes; ++p) {
 		const int vm = (indexMode && p == 0) ? mgpusort::kValueIndex : numArrays;
 		mgpusort::PassBuffers buf = {};
@@ -183,15 +171,8 @@ extern "C" sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t d, CUstream cuStream
 			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
 			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
 		}
-		if(s.epoch >= kMaxEpoch) {
-			if(cudaMemsetAsync(status, 0, statusBytes, stream) != cudaSuccess) {
-				cudaGetLastError();
-				return SORT_STATUS_DEVICE_ERROR;
-			}
-			s.epoch = 0;
-		}
-		ce = mgpusort::launch_pass(buf, vm, n, p, plan, ctrl, status, ++s.epoch,
-			bulk, -1, nullptr, stream);
+		ce = mgpusort::launch_pass(buf, vm, n, p, plan, ctrl, passScratch, bulk, -1,
+			nullptr, s.numSMs, stream);
 		if(ce != cudaSuccess) return SORT_STATUS_LAUNCH_ERROR;
 		swap_buffers(d);
 	}

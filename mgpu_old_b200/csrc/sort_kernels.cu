@@ -40,48 +40,42 @@ struct UpsweepArgs {
 	volatile unsigned* hostError;
 };
 
-// Count nValid (a prefix of) keys into a shared histogram. Runs of equal
-// digits in a thread's keys are merged into one atomic, which keeps skewed
-// digits (e.g. all-zero high bytes) from serialising on one counter.
+// Each bin of the upsweep's shared histogram has kUpCopies counters, one per
+// lane class (lane % kUpCopies), in consecutive words: lanes of a warp that
+// hit the same bin in one instruction mostly update different words (in
+// different banks), which keeps skewed digits from serialising the atomics.
+constexpr int kUpCopies = 4;
+
 __device__ __forceinline__ void count_digits(unsigned* hist,
 	const unsigned (&k)[kUpKeysPerThread], int nValid, int shift,
-	unsigned mask) {
-	unsigned cur = (k[0] >> shift) & mask;
-	unsigned run = 0;
+	unsigned mask, int copy) {
 #pragma unroll
-	for(int i = 0; i < kUpKeysPerThread; ++i) {
-		if(i < nValid) {
-			unsigned d = (k[i] >> shift) & mask;
-			if(d != cur) {
-				atomicAdd(&hist[cur], run);
-				cur = d;
-				run = 1;
-			} else ++run;
-		}
-	}
-	if(run) atomicAdd(&hist[cur], run);
+	for(int i = 0; i < kUpKeysPerThread; ++i)
+		if(i < nValid)
+			atomicAdd(&hist[((k[i] >> shift) & mask) * kUpCopies + copy], 1u);
 }
 
 __global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 	const UpsweepArgs a) {
 
-	__shared__ unsigned sHist[kMaxBins];
+	__shared__ unsigned sHist[kMaxBins * kUpCopies];
 	__shared__ unsigned sScan[kUpThreads / 32];
 	__shared__ unsigned sLast;
 
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
+	const int copy = lane & (kUpCopies - 1);
 	const int totalBins = a.plan.totalBins;
 	const int numPasses = a.plan.numPasses;
 
-	for(int i = tid; i < totalBins; i += kUpThreads) sHist[i] = 0;
+	for(int i = tid; i < totalBins * kUpCopies; i += kUpThreads) sHist[i] = 0;
 	__syncthreads();
 
 	auto count_all = [&](const unsigned (&k)[kUpKeysPerThread], int nValid) {
 		for(int p = 0; p < numPasses; ++p)
-			count_digits(sHist + a.plan.binBase[p], k, nValid, a.plan.shift[p],
-				(1u << a.plan.width[p]) - 1);
+			count_digits(sHist + a.plan.binBase[p] * kUpCopies, k, nValid,
+				a.plan.shift[p], (1u << a.plan.width[p]) - 1, copy);
 	};
 
 	// Full chunks with 16-byte loads, the next chunk's loads in flight while
@@ -136,7 +130,9 @@ __global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 	__syncthreads();
 
 	for(int i = tid; i < totalBins; i += kUpThreads) {
-		unsigned c = sHist[i];
+		unsigned c = 0;
+#pragma unroll
+		for(int j = 0; j < kUpCopies; ++j) c += sHist[i * kUpCopies + j];
 		if(c) atomicAdd(&a.ctrl->hist[i], c);
 	}
 	__threadfence();
@@ -171,384 +167,516 @@ __global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 }
 
 ////////////////////////////////////////////////////////////////////////////////
-// Onesweep pass.
+// One pass = count + scan + sort over a range partition.
+//
+// The tiles of a pass are split into R ranges of consecutive tiles, one per
+// CTA of the sort kernel. count_kernel builds each range's digit histogram
+// (one read of the keys); scan_kernel turns them, per digit, into the
+// exclusive prefix over ranges and the digit's total; sort_kernel CTA r
+// starts each digit at (keys with smaller digits in the whole array) + (keys
+// with this digit in ranges before r) and walks its tiles in order: stable
+// rank of the tile, reorder into digit runs in shared memory, run-wise
+// stores, then advance each digit's offset by the tile's count. No tile
+// waits for another tile, and each CTA copies its next tile in while it sorts
+// the current one. This is the reference's count -> histogram scan -> sort
+// structure (sort/src/mgpusort/mgpusort.cpp:421-516) with per-range instead
+// of per-block counts.
 
-struct PassArgs {
-	PassBuffers buf;
-	const unsigned* digitOffsets;   // exclusive global start of each digit
-	const unsigned* trivial;        // nonzero: one digit only, pass = copy
-	unsigned* tileCounter;
-	unsigned long long* status;     // [numTiles][256] lookback words
-	unsigned* devError;
-	volatile unsigned* hostError;
-	int n;
+// Consecutive tiles [first_tile(r), first_tile(r + 1)) form range r.
+struct RangeSplit {
 	int numTiles;
+	int numRanges;
+	int tilesLo;    // tiles per range; the first `extra` ranges have one more
+	int extra;
+	__host__ __device__ __forceinline__ int first_tile(int r) const {
+		return r * tilesLo + (r < extra ? r : extra);
+	}
+};
+
+constexpr int kTileElements = 4096;
+constexpr int kCountThreads = 512;
+
+struct CountArgs {
+	const unsigned* keys;
+	int n;
 	int shift;
 	int width;
-	unsigned epoch;
-	int useBulk;
-	int failTile;                   // tile that skips publishing; -1: none
+	int vecOk;
+	RangeSplit split;
+	unsigned* rangeCounts;          // [256][R], digit-major
 };
 
-// Lookback word: epoch (30 bits) | flag (2 bits) | count (32 bits). A word
-// whose epoch is not the current pass's is treated as not yet published, so
-// the status array never needs clearing between passes.
-constexpr unsigned long long kFlagAggregate = 1ull << 32;
-constexpr unsigned long long kFlagInclusive = 2ull << 32;
+__global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a) {
+	__shared__ unsigned sHist[kDigitBins * kUpCopies];
+	const int tid = threadIdx.x;
+	const int copy = tid & (kUpCopies - 1);
+	const int r = blockIdx.x;
+	const unsigned mask = (1u << a.width) - 1;
+	const int shift = a.shift;
 
-template<int VM> struct PassConfig {
+	for(int i = tid; i < kDigitBins * kUpCopies; i += kCountThreads) sHist[i] = 0;
+	__syncthreads();
+
+	const long long begin = (long long)a.split.first_tile(r) * kTileElements;
+	const long long end = min((long long)a.n,
+		(long long)a.split.first_tile(r + 1) * kTileElements);
+	auto add = [&](unsigned k) {
+		atomicAdd(&sHist[((k >> shift) & mask) * kUpCopies + copy], 1u);
+	};
+	long long done = begin;
+	if(a.vecOk) {
+		// begin is a multiple of the tile size: 16-byte aligned.
+		const uint4* src = reinterpret_cast<const uint4*>(a.keys + begin);
+		const int nvec = (int)((end - begin) / 4);
+		constexpr int U = 4;
+		int i = tid;
+		for(; i + (U - 1) * kCountThreads < nvec; i += U * kCountThreads) {
+			uint4 q[U];
+#pragma unroll
+			for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + i + u * kCountThreads);
+#pragma unroll
+			for(int u = 0; u < U; ++u) {
+				add(q[u].x);
+				add(q[u].y);
+				add(q[u].z);
+				add(q[u].w);
+			}
+		}
+		for(; i < nvec; i += kCountThreads) {
+			const uint4 q = ld_stream_u4(src + i);
+			add(q.x);
+			add(q.y);
+			add(q.z);
+			add(q.w);
+		}
+		done = begin + 4ll * nvec;
+	}
+	for(long long e = done + tid; e < end; e += kCountThreads) add(a.keys[e]);
+	__syncthreads();
+
+	if(tid < kDigitBins) {
+		unsigned c = 0;
+#pragma unroll
+		for(int j = 0; j < kUpCopies; ++j) c += sHist[tid * kUpCopies + j];
+		a.rangeCounts[(size_t)tid * a.split.numRanges + r] = c;
+	}
+}
+
+struct ScanArgs {
+	const unsigned* rangeCounts;    // [256][R]
+	unsigned* rangeOffsets;         // [256][R]: exclusive over ranges
+	unsigned* totals;               // [256]
+	int numRanges;
+};
+
+// One warp per digit: exclusive scan of the digit's range counts.
+__global__ void __launch_bounds__(256) scan_kernel(const ScanArgs a) {
+	const int lane = threadIdx.x & 31;
+	const int d = blockIdx.x * 8 + (threadIdx.x >> 5);
+	const unsigned* in = a.rangeCounts + (size_t)d * a.numRanges;
+	unsigned* out = a.rangeOffsets + (size_t)d * a.numRanges;
+	unsigned carry = 0;
+	for(int base = 0; base < a.numRanges; base += 32) {
+		const int r = base + lane;
+		const unsigned v = r < a.numRanges ? in[r] : 0u;
+		const unsigned incl = warp_inclusive_scan(v, lane);
+		if(r < a.numRanges) out[r] = carry + incl - v;
+		carry += __shfl_sync(0xffffffffu, incl, 31);
+	}
+	if(lane == 0) a.totals[d] = carry;
+}
+
+struct SortArgs {
+	PassBuffers buf;
+	const unsigned* rangeOffsets;   // [256][R]
+	const unsigned* totals;         // [256]
+	unsigned* devError;
+	volatile unsigned* hostError;
+	RangeSplit split;
+	int n;
+	int shift;
+	int width;
+	int useBulk;
+	int failTile;                   // tile whose CTA runs a wait out; -1: none
+};
+
+template<int VM> struct SortConfig {
 	static constexpr int kThreads = 256;
 	static constexpr int kItems = 16;
-	static constexpr int kMinBlocks = 4;
+	static constexpr int kMinBlocks = 3;
+	// Key tiles staged per CTA: with two, the next tile's keys are copied in
+	// while this tile is sorted.
+	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
 };
 
-template<int VM> struct PassLayout {
-	static constexpr int NT = PassConfig<VM>::kThreads;
-	static constexpr int IPT = PassConfig<VM>::kItems;
+template<int VM> struct SortLayout {
+	static constexpr int NT = SortConfig<VM>::kThreads;
+	static constexpr int IPT = SortConfig<VM>::kItems;
 	static constexpr int TILE = NT * IPT;
 	static constexpr int NW = NT / 32;
-	// Value staging buffers: index mode writes its generated indices into
-	// one, value arrays are double-buffered.
-	static constexpr int NSTAGE = VM >= 2 ? 2 : (VM == 0 ? 0 : 1);
+	static constexpr int KSLOTS = SortConfig<VM>::kKeySlots;
+	static constexpr int NV = VM > 0 ? VM : 0;
+	// One value buffer holds the first value array (or the generated
+	// indices); with more arrays, each further one is copied into the stream
+	// buffer while the one before it is reordered in the value buffer.
+	static constexpr int NVBUF = VM == 0 ? 0 : 1;
+	static constexpr int NSTREAM = NV >= 2 ? 1 : 0;
 	// Word offsets into dynamic shared memory.
 	static constexpr int kKeys = 0;
-	static constexpr int kVals = kKeys + TILE;
-	static constexpr int kWarpHist = kVals + NSTAGE * TILE;
+	static constexpr int kVals = kKeys + KSLOTS * TILE;
+	static constexpr int kStream = kVals + NVBUF * TILE;
+	static constexpr int kWarpHist = kStream + NSTREAM * TILE;
 	static constexpr int kDigStart = kWarpHist + NW * kDigitBins;
-	static constexpr int kScatter = kDigStart + kDigitBins;
+	static constexpr int kCount = kDigStart + kDigitBins;
+	static constexpr int kRunning = kCount + kDigitBins;
+	static constexpr int kScatter = kRunning + kDigitBins;
 	static constexpr int kScan = kScatter + kDigitBins;
 	static constexpr int kBar = kScan + 32;          // 8-byte aligned: even
-	static constexpr int kTile = kBar + 2 * 4;
-	static constexpr int kWords = kTile + 4;
+	static constexpr int kWords = kBar + 2 * 6;       // 6 mbarriers
 	static constexpr size_t kBytes = sizeof(unsigned) * kWords;
 	static_assert(kBar % 2 == 0, "mbarriers need 8-byte alignment");
+	static_assert(TILE == kTileElements, "count and sort kernels share tiles");
 };
 
-// Identity pass (all keys share the digit): copy the tile through.
-template<int VM>
-__device__ __forceinline__ void copy_tile(const PassArgs& a, long long start,
-	int count) {
-	constexpr int NT = PassLayout<VM>::NT;
-	const int tid = threadIdx.x;
-	for(int i = tid; i < count; i += NT) {
-		a.buf.keysOut[start + i] = a.buf.keysIn[start + i];
-		if constexpr(VM == kValueIndex)
-			a.buf.valsOut[0][start + i] = (unsigned)(start + i);
+// Peers of an 8-bit digit: the lanes of the warp whose digit equals this
+// lane's. From the eight ballots of the digit bits, lane l builds two
+// entries of two 16-entry tables: the lanes whose low nibble is l & 15 and
+// the lanes whose high nibble is l & 15 (nClear[k] is all ones where bit k of
+// l & 15 is clear, so ballot ^ nClear[k] is the set of lanes agreeing with
+// that bit). A lane's peers are the AND of the low-table entry for its low
+// nibble and the high-table entry for its high nibble, fetched by shuffle.
+__device__ __forceinline__ unsigned match_digit8(unsigned d,
+	const unsigned (&nClear)[4]) {
+	unsigned bal[8];
 #pragma unroll
-		for(int v = 0; v < (VM > 0 ? VM : 0); ++v)
-			a.buf.valsOut[v][start + i] = a.buf.valsIn[v][start + i];
+	for(int b = 0; b < 8; ++b) bal[b] = __ballot_sync(0xffffffffu, d & (1u << b));
+	unsigned lo = bal[0] ^ nClear[0];
+	unsigned hi = bal[4] ^ nClear[0];
+#pragma unroll
+	for(int k = 1; k < 4; ++k) {
+		lo &= bal[k] ^ nClear[k];
+		hi &= bal[4 + k] ^ nClear[k];
 	}
+	return __shfl_sync(0xffffffffu, lo, d & 15u) & __shfl_sync(0xffffffffu, hi, d >> 4);
 }
 
-// Lanes of the warp whose 8-bit digit equals this lane's, from one ballot per
-// digit bit (a lane keeps the ballot where its bit is set, the complement
-// where it is clear).
-__device__ __forceinline__ unsigned match_digit8(unsigned d) {
-	unsigned peers = 0xffffffffu;
-#pragma unroll
-	for(int b = 0; b < 8; ++b) {
-		const bool set = (d >> b) & 1u;
-		const unsigned bal = __ballot_sync(0xffffffffu, set);
-		peers &= set ? bal : ~bal;
-	}
-	return peers;
+// Stable warp rank of one item: the highest peer adds the group's size to
+// the warp's running count of the digit; the old count, broadcast, is the
+// group's base. Returns (digit << 16) | rank within the warp.
+__device__ __forceinline__ unsigned rank_item(unsigned d, unsigned* warpHist,
+	int lane, unsigned ltMask, const unsigned (&nClear)[4]) {
+	const unsigned peers = match_digit8(d, nClear);
+	const int leader = 31 - __clz(peers);
+	unsigned base = 0;
+	if(lane == leader) base = atomicAdd(&warpHist[d], (unsigned)__popc(peers));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	// Orders this item's counter update before the next item's.
+	__syncwarp();
+	return (d << 16) | (base + __popc(peers & ltMask));
 }
 
-// Decoupled lookback of one digit: sum the counts of the tiles before `tile`
-// back to the nearest one that published an inclusive prefix. Reads up to
-// four predecessors per step so that a walk over published aggregates costs
-// one memory round trip per four tiles.
-__device__ __forceinline__ unsigned lookback_digit(
-	const unsigned long long* status, int tile, int digit, unsigned epoch,
-	bool* timedOut) {
-	unsigned excl = 0;
-	int j = tile - 1;
-	WaitBudget budget;
-	while(true) {
-		unsigned long long w[4];
+__device__ __forceinline__ void stage_tile(unsigned* dst, const unsigned* src,
+	unsigned bytes, uint64_t* bar) {
+	mbar_arrive_expect_tx(bar, bytes);
+	bulk_load(dst, src, bytes, bar);
+}
+
+// Rank the staged tile's keys (warp-striped: item i of lane l in warp w is
+// tile element w*32*IPT + i*32 + l, so (item, lane) order is input order per
+// warp). In a partial tile the elements past `count` get digit 255: they
+// rank after every real key and are never stored.
+template<int IPT, bool FULL>
+__device__ __forceinline__ void rank_tile(const unsigned* sKeys, unsigned* myHist,
+	int warpBase, int lane, int count, int shift, unsigned mask, unsigned ltMask,
+	const unsigned (&nClear)[4], unsigned (&rank)[IPT]) {
 #pragma unroll
-		for(int k = 0; k < 4; ++k)
-			w[k] = j - k >= 0
-				? ld_relaxed_u64(status + (size_t)(j - k) * kDigitBins + digit) : 0ull;
-		int consumed = 0;
-		bool done = false, stalled = false;
-#pragma unroll
-		for(int k = 0; k < 4; ++k) {
-			if(done || stalled) continue;
-			const unsigned long long flag = w[k] & (3ull << 32);
-			if(j - k < 0 || (w[k] >> 34) != epoch || !flag) {
-				stalled = true;
-				continue;
-			}
-			excl += (unsigned)w[k];
-			++consumed;
-			if(flag == kFlagInclusive) done = true;
-		}
-		if(done) break;
-		j -= consumed;
-		if(consumed) budget = WaitBudget();
-		else if(!budget.poll()) {
-			*timedOut = true;
-			break;
-		}
+	for(int i = 0; i < IPT; ++i) {
+		const int idx = warpBase + i * 32 + lane;
+		unsigned d = (sKeys[idx] >> shift) & mask;
+		if(!FULL && idx >= count) d = kDigitBins - 1;
+		rank[i] = rank_item(d, myHist, lane, ltMask, nClear);
 	}
-	return excl;
 }
 
 template<int VM>
-__global__ void __launch_bounds__(PassLayout<VM>::NT, PassConfig<VM>::kMinBlocks)
-onesweep_kernel(const PassArgs a) {
+__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
+sort_kernel(const SortArgs a) {
 
-	using L = PassLayout<VM>;
+	using L = SortLayout<VM>;
 	constexpr int NT = L::NT;
 	constexpr int IPT = L::IPT;
 	constexpr int TILE = L::TILE;
 	constexpr int NW = L::NW;
-	constexpr int NV = VM > 0 ? VM : 0;
-	// Value arrays (or generated indices) reordered in shared memory before
-	// the lookback; the rest stream through the staging buffers after it.
-	constexpr int NPRE = VM == kValueIndex ? 1 : (NV < 2 ? NV : 2);
+	constexpr int NV = L::NV;
+	constexpr int KSLOTS = L::KSLOTS;
+	constexpr unsigned kTileBytes = TILE * 4;
 
 	extern __shared__ __align__(128) unsigned smem[];
-	unsigned* sKeys = smem + L::kKeys;
 	unsigned* sVals = smem + L::kVals;
+	unsigned* sStream = smem + L::kStream;
 	unsigned* sWarpHist = smem + L::kWarpHist;
-	unsigned* sDigStart = smem + L::kDigStart;
+	unsigned* sRunning = smem + L::kRunning;
 	int* sScatter = reinterpret_cast<int*>(smem + L::kScatter);
 	unsigned* sScan = smem + L::kScan;
+	// mbarriers: [0..1] key slots, [2] value buffer, [3] stream buffer,
+	// [5] injected-fault wait (never completed).
 	uint64_t* sBar = reinterpret_cast<uint64_t*>(smem + L::kBar);
-	unsigned* sTile = smem + L::kTile;
 
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
+	const int warpBase = warp * 32 * IPT;
+	const int r = blockIdx.x;
+	const int t0 = a.split.first_tile(r);
+	const int t1 = a.split.first_tile(r + 1);
+	const int R = a.split.numRanges;
+
+	// Each digit starts at the keys with smaller digits in the whole array
+	// plus the keys with this digit in the ranges before this one.
+	const unsigned total = tid < kDigitBins ? a.totals[tid] : 0u;
+	const unsigned inclTotal = warp_inclusive_scan(total, lane);
+	if(lane == 31 && tid < kDigitBins) sScan[warp] = inclTotal;
+	const int nonEmpty = __syncthreads_count(tid < kDigitBins && total != 0);
+	if(tid < kDigitBins) {
+		unsigned prefix = 0;
+		for(int w = 0; w < warp; ++w) prefix += sScan[w];
+		sRunning[tid] = prefix + inclTotal - total + a.rangeOffsets[(size_t)tid * R + r];
+	}
+
+	if(nonEmpty <= 1) {
+		// Every key has the same digit: the pass is the identity.
+		const long long b = (long long)t0 * TILE;
+		const long long e = min((long long)a.n, (long long)t1 * TILE);
+		for(long long i = b + tid; i < e; i += NT) {
+			a.buf.keysOut[i] = a.buf.keysIn[i];
+			if constexpr(VM == kValueIndex) a.buf.valsOut[0][i] = (unsigned)i;
+#pragma unroll
+			for(int v = 0; v < NV; ++v) a.buf.valsOut[v][i] = a.buf.valsIn[v][i];
+		}
+		return;
+	}
+
+	auto tile_is_bulk = [&](int t) {
+		return a.useBulk && (long long)(t + 1) * TILE <= a.n;
+	};
 
 	if(tid == 0) {
-		unsigned t = atomicAdd(a.tileCounter, 1u);
-		// Every CTA of this launch has drawn its id once this one has the
-		// last: re-arm the counter for the next launch.
-		if(t == (unsigned)a.numTiles - 1) *a.tileCounter = 0;
-		sTile[0] = t;
-		sTile[1] = *a.trivial;
-		if(a.useBulk) {
-			mbar_init(&sBar[0], 1);
-			mbar_init(&sBar[1], 1);
-			mbar_init(&sBar[2], 1);
-			fence_mbar_init();
+		for(int i = 0; i < 6; ++i) mbar_init(&sBar[i], 1);
+		fence_mbar_init();
+		if(t0 < t1 && tile_is_bulk(t0)) {
+			stage_tile(smem + L::kKeys, a.buf.keysIn + (size_t)t0 * TILE, kTileBytes,
+				&sBar[0]);
+			if constexpr(NV >= 1)
+				stage_tile(sVals, a.buf.valsIn[0] + (size_t)t0 * TILE, kTileBytes, &sBar[2]);
 		}
 	}
 	for(int i = tid; i < NW * kDigitBins; i += NT) sWarpHist[i] = 0;
 	__syncthreads();
 
-	const int tile = (int)sTile[0];
-	const long long tileStart = (long long)tile * TILE;
-	const int count = (int)min((long long)TILE, (long long)a.n - tileStart);
-
-	if(sTile[1]) {
-		copy_tile<VM>(a, tileStart, count);
-		return;
-	}
-
-	const bool bulk = a.useBulk && count == TILE;
-	if(bulk && tid == 0) {
-		mbar_arrive_expect_tx(&sBar[0], TILE * 4);
-		bulk_load(sKeys, a.buf.keysIn + tileStart, TILE * 4, &sBar[0]);
-		if constexpr(NV >= 1) {
-			mbar_arrive_expect_tx(&sBar[1], TILE * 4);
-			bulk_load(sVals, a.buf.valsIn[0] + tileStart, TILE * 4, &sBar[1]);
-		}
-		if constexpr(NV >= 2) {
-			mbar_arrive_expect_tx(&sBar[2], TILE * 4);
-			bulk_load(sVals + TILE, a.buf.valsIn[1] + tileStart, TILE * 4,
-				&sBar[2]);
-		}
-	}
-
-	// Keys in warp-striped order: item i of lane l in warp w is tile element
-	// w*32*IPT + i*32 + l, so (item, lane) order is input order per warp.
-	const int warpBase = warp * 32 * IPT;
-	unsigned keys[IPT];
-	if(bulk) {
-		if(!mbar_wait_bounded(&sBar[0], 0))
-			report_error(a.devError, a.hostError, kErrBarrierTimeout);
-#pragma unroll
-		for(int i = 0; i < IPT; ++i) keys[i] = sKeys[warpBase + i * 32 + lane];
-	} else {
-#pragma unroll
-		for(int i = 0; i < IPT; ++i) {
-			int idx = warpBase + i * 32 + lane;
-			keys[i] = idx < count ? a.buf.keysIn[tileStart + idx] : 0xffffffffu;
-		}
-	}
-
 	const unsigned mask = (1u << a.width) - 1;
 	const int shift = a.shift;
-	// Padding of a partial tile gets digit 255: it ranks after every real
-	// key (it is last in input order and 255 is the last bin) and is never
-	// stored.
-	auto digit_of = [&](int i) -> unsigned {
-		int idx = warpBase + i * 32 + lane;
-		return idx < count ? (keys[i] >> shift) & mask : (kDigitBins - 1);
-	};
-
-	// Stable rank within the warp: peers with the same digit are ranked by
-	// lane, items in order. The highest peer adds the group to the warp's
-	// running count of the digit; the atomic's old value, broadcast, is the
-	// group's base. The shuffle orders each item's update before the next.
-	unsigned* myHist = sWarpHist + warp * kDigitBins;
 	const unsigned ltMask = lanemask_lt();
-	unsigned rank[IPT];
+	unsigned nClear[4];
 #pragma unroll
-	for(int i = 0; i < IPT; ++i) {
-		const unsigned d = digit_of(i);
-		const unsigned peers = match_digit8(d);
-		const int leader = 31 - __clz(peers);
-		unsigned base = 0;
-		if(lane == leader) base = atomicAdd(&myHist[d], (unsigned)__popc(peers));
-		base = __shfl_sync(0xffffffffu, base, leader);
-		rank[i] = base + __popc(peers & ltMask);
-	}
-	__syncthreads();
+	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
+	unsigned phase = 0;    // bit s: key slot s; bit 2: value buffer; bit 3: stream
+	int slot = 0;
 
-	// Per digit: exclusive offsets of the warps, and the tile's count.
-	unsigned total = 0;
-	if(tid < kDigitBins) {
-#pragma unroll
-		for(int w = 0; w < NW; ++w) {
-			unsigned c = sWarpHist[w * kDigitBins + tid];
-			sWarpHist[w * kDigitBins + tid] = total;
-			total += c;
-		}
-	}
-	const unsigned incl = warp_inclusive_scan(total, lane);
-	if(lane == 31 && tid < kDigitBins) sScan[warp] = incl;
-	__syncthreads();
+	for(int tile = t0; tile < t1; ++tile) {
+		unsigned* sKeys = smem + L::kKeys + slot * TILE;
+		const long long tileStart = (long long)tile * TILE;
+		const int count = (int)min((long long)TILE, (long long)a.n - tileStart);
+		const bool bulk = tile_is_bulk(tile);
+		const int next = tile + 1;
 
-	// Publish this tile's digit counts as soon as they are known.
-	const unsigned long long epochBits = (unsigned long long)a.epoch << 34;
-	unsigned digStart = 0;
-	unsigned mine = 0;
-	if(tid < kDigitBins) {
-		unsigned prefix = 0;
-		for(int w = 0; w < warp; ++w) prefix += sScan[w];
-		digStart = prefix + incl - total;
-		sDigStart[tid] = digStart;
-		mine = total;
-		if(tid == kDigitBins - 1) mine -= TILE - count;
-		if(tid <= (int)mask && tile != a.failTile) {
-			unsigned long long* st = a.status + (size_t)tile * kDigitBins + tid;
-			st_relaxed_u64(st, epochBits | (tile == 0 ? kFlagInclusive : kFlagAggregate)
-				| mine);
-		}
-	}
-	__syncthreads();
-
-	// Reorder the tile in shared memory into digit runs: keys, then the
-	// value arrays whose tiles are already staged (or generated indices).
-#pragma unroll
-	for(int i = 0; i < IPT; ++i) {
-		const unsigned d = digit_of(i);
-		rank[i] += sDigStart[d] + sWarpHist[warp * kDigitBins + d];
-		sKeys[rank[i]] = keys[i];
-	}
-	if constexpr(VM == kValueIndex) {
-#pragma unroll
-		for(int i = 0; i < IPT; ++i)
-			sVals[rank[i]] = (unsigned)(tileStart + warpBase + i * 32 + lane);
-	}
-#pragma unroll
-	for(int v = 0; v < (VM > 0 ? NPRE : 0); ++v) {
-		unsigned vals[IPT];
-		if(bulk) {
-			if(!mbar_wait_bounded(&sBar[1 + v], 0))
-				report_error(a.devError, a.hostError, kErrBarrierTimeout);
-#pragma unroll
-			for(int i = 0; i < IPT; ++i) vals[i] = sVals[v * TILE + warpBase + i * 32 + lane];
-		} else {
-#pragma unroll
-			for(int i = 0; i < IPT; ++i) {
-				int idx = warpBase + i * 32 + lane;
-				vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
-			}
-		}
-		__syncthreads();
-#pragma unroll
-		for(int i = 0; i < IPT; ++i) sVals[v * TILE + rank[i]] = vals[i];
-	}
-
-	// Global offsets: the digit's start over the whole array plus the counts
-	// of the tiles before this one.
-	if(tid <= (int)mask) {
-		unsigned excl = 0;
-		if(tile == a.failTile) {
-			// Injected fault (tests only): this tile never publishes, so the
-			// tiles after it run their bounded waits out.
-			if(tid == 0) report_error(a.devError, a.hostError, kErrInjected);
-		} else if(tile > 0) {
-			bool timedOut = false;
-			excl = lookback_digit(a.status, tile, tid, a.epoch, &timedOut);
-			if(timedOut) report_error(a.devError, a.hostError, kErrLookbackTimeout);
-			st_relaxed_u64(a.status + (size_t)tile * kDigitBins + tid,
-				epochBits | kFlagInclusive | (excl + mine));
-		}
-		sScatter[tid] = (int)(a.digitOffsets[tid] + excl - digStart);
-	}
-	__syncthreads();
-
-	// Write each run to its global position: element p of the reordered tile
-	// goes to scatter[digit] + p, consecutive p -> consecutive addresses.
-#pragma unroll
-	for(int j = 0; j < IPT; ++j) {
-		const int p = j * NT + tid;
-		if(p < count) {
-			const unsigned k = sKeys[p];
-			const int dst = sScatter[(k >> shift) & mask] + p;
-			a.buf.keysOut[dst] = k;
-			if constexpr(VM == kValueIndex) a.buf.valsOut[0][dst] = sVals[p];
-#pragma unroll
-			for(int v = 0; v < (VM > 0 ? NPRE : 0); ++v)
-				a.buf.valsOut[v][dst] = sVals[v * TILE + p];
-		}
-	}
-
-	// Remaining value arrays stream through the two staging buffers.
-#pragma unroll
-	for(int v = NPRE; v < NV; ++v) {
-		const int stage = v & 1;
-		unsigned* buf = sVals + stage * TILE;
-		// Everyone is done with this staging buffer (its last reader was the
-		// store of array v - 2): refill it.
-		__syncthreads();
-		if(bulk && tid == 0) {
+		// The next tile's keys go into the other slot (free since the end of
+		// the previous iteration) while this one is sorted.
+		if(KSLOTS == 2 && tid == 0 && next < t1 && tile_is_bulk(next)) {
 			fence_proxy_async_smem();
-			mbar_arrive_expect_tx(&sBar[1 + stage], TILE * 4);
-			bulk_load(buf, a.buf.valsIn[v] + tileStart, TILE * 4, &sBar[1 + stage]);
+			stage_tile(smem + L::kKeys + (slot ^ 1) * TILE,
+				a.buf.keysIn + (size_t)next * TILE, kTileBytes, &sBar[slot ^ 1]);
 		}
-		unsigned vals[IPT];
+
+		unsigned* myHist = sWarpHist + warp * kDigitBins;
+		unsigned rank[IPT];
 		if(bulk) {
-			if(!mbar_wait_bounded(&sBar[1 + stage], (v >> 1) & 1))
+			if(!mbar_wait_bounded(&sBar[slot], (phase >> slot) & 1u))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
+			phase ^= 1u << slot;
+			rank_tile<IPT, true>(sKeys, myHist, warpBase, lane, count, shift, mask,
+				ltMask, nClear, rank);
+		} else {
+			// Plain loads (a partial tile, or buffers that are not 16-byte
+			// aligned): stage the keys and the first value array by hand.
+			for(int i = tid; i < TILE; i += NT) {
+				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
+				if constexpr(NV >= 1)
+					sVals[i] = i < count ? a.buf.valsIn[0][tileStart + i] : 0u;
+			}
+			__syncthreads();
+			rank_tile<IPT, false>(sKeys, myHist, warpBase, lane, count, shift, mask,
+				ltMask, nClear, rank);
+		}
+		__syncthreads();
+
+		// Per digit: the tile's count, its exclusive digit start, and for every
+		// warp the position where its run of the digit begins in the reordered
+		// tile (digit start + counts of the warps before it).
+		unsigned c[NW];
+		unsigned tileTotal = 0;
+		if(tid < kDigitBins) {
 #pragma unroll
-			for(int i = 0; i < IPT; ++i) vals[i] = buf[warpBase + i * 32 + lane];
+			for(int w = 0; w < NW; ++w) {
+				c[w] = sWarpHist[w * kDigitBins + tid];
+				tileTotal += c[w];
+			}
+		}
+		const unsigned incl = warp_inclusive_scan(tileTotal, lane);
+		if(lane == 31 && tid < kDigitBins) sScan[warp] = incl;
+		__syncthreads();
+		if(tid < kDigitBins) {
+			unsigned prefix = 0;
+			for(int w = 0; w < warp; ++w) prefix += sScan[w];
+			const unsigned digStart = prefix + incl - tileTotal;
+			unsigned run = digStart;
+#pragma unroll
+			for(int w = 0; w < NW; ++w) {
+				sWarpHist[w * kDigitBins + tid] = run;
+				run += c[w];
+			}
+			// Global position of element p of digit tid's run: scatter + p.
+			// Padding is only ever in digit 255 and is not counted.
+			const unsigned mine = tileTotal - (tid == kDigitBins - 1 ? TILE - count : 0);
+			const unsigned g = sRunning[tid];
+			sScatter[tid] = (int)(g - digStart);
+			sRunning[tid] = g + mine;
+		}
+
+		// Every warp's keys leave shared memory for registers before the tile
+		// is reordered in place.
+		unsigned keys[IPT];
+#pragma unroll
+		for(int i = 0; i < IPT; ++i) keys[i] = sKeys[warpBase + i * 32 + lane];
+		__syncthreads();
+
+		// Reorder the tile into digit runs in shared memory: keys in place,
+		// then the first value array (or the generated indices).
+#pragma unroll
+		for(int i = 0; i < IPT; ++i) {
+			rank[i] = (rank[i] & 0xffffu) + sWarpHist[warp * kDigitBins + (rank[i] >> 16)];
+			sKeys[rank[i]] = keys[i];
+		}
+		if constexpr(VM == kValueIndex) {
+#pragma unroll
+			for(int i = 0; i < IPT; ++i)
+				sVals[rank[i]] = (unsigned)(tileStart + warpBase + i * 32 + lane);
+		}
+		if constexpr(NV >= 1) {
+			unsigned vals[IPT];
+			if(bulk) {
+				if(!mbar_wait_bounded(&sBar[2], (phase >> 2) & 1u))
+					report_error(a.devError, a.hostError, kErrBarrierTimeout);
+				phase ^= 1u << 2;
+			}
+#pragma unroll
+			for(int i = 0; i < IPT; ++i) vals[i] = sVals[warpBase + i * 32 + lane];
+			__syncthreads();
+#pragma unroll
+			for(int i = 0; i < IPT; ++i) sVals[rank[i]] = vals[i];
+		}
+		if constexpr(NV >= 2) {
+			// The second value array heads for the stream buffer now.
+			if(bulk && tid == 0) {
+				fence_proxy_async_smem();
+				stage_tile(sStream, a.buf.valsIn[1] + tileStart, kTileBytes, &sBar[3]);
+			}
+		}
+		if(tile == a.failTile && tid == 0) {
+			// Injected fault (tests only): wait on a barrier that nothing
+			// completes, so the bounded wait runs out and is reported.
+			if(!mbar_wait_bounded(&sBar[5], 0))
+				report_error(a.devError, a.hostError, kErrInjected);
+		}
+		__syncthreads();
+
+		// Write each run to its global position: element p of the reordered
+		// tile goes to scatter[digit] + p; consecutive p, consecutive addresses.
+		if(count == TILE) {
+#pragma unroll
+			for(int j = 0; j < IPT; ++j) {
+				const int p = j * NT + tid;
+				const unsigned k = sKeys[p];
+				const int dst = sScatter[(k >> shift) & mask] + p;
+				a.buf.keysOut[dst] = k;
+				if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+			}
 		} else {
 #pragma unroll
-			for(int i = 0; i < IPT; ++i) {
-				int idx = warpBase + i * 32 + lane;
-				vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
+			for(int j = 0; j < IPT; ++j) {
+				const int p = j * NT + tid;
+				if(p < count) {
+					const unsigned k = sKeys[p];
+					const int dst = sScatter[(k >> shift) & mask] + p;
+					a.buf.keysOut[dst] = k;
+					if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+				}
 			}
 		}
-		__syncthreads();
+
+		// Value arrays 2..V: array v arrives in the stream buffer (requested
+		// while array v - 1 was reordered), is read out, array v + 1 is
+		// requested into the stream buffer, and array v is reordered in the
+		// value buffer and stored.
 #pragma unroll
-		for(int i = 0; i < IPT; ++i) buf[rank[i]] = vals[i];
-		__syncthreads();
+		for(int v = 1; v < NV; ++v) {
+			unsigned vals[IPT];
+			if(bulk) {
+				if(!mbar_wait_bounded(&sBar[3], (phase >> 3) & 1u))
+					report_error(a.devError, a.hostError, kErrBarrierTimeout);
+				phase ^= 1u << 3;
 #pragma unroll
-		for(int j = 0; j < IPT; ++j) {
-			const int p = j * NT + tid;
-			if(p < count) {
-				const int dst = sScatter[(sKeys[p] >> shift) & mask] + p;
-				a.buf.valsOut[v][dst] = buf[p];
+				for(int i = 0; i < IPT; ++i) vals[i] = sStream[warpBase + i * 32 + lane];
+			} else {
+#pragma unroll
+				for(int i = 0; i < IPT; ++i) {
+					const int idx = warpBase + i * 32 + lane;
+					vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
+				}
+			}
+			// Everyone has read the stream buffer and finished the stores
+			// that read the value buffer.
+			__syncthreads();
+			if(bulk && tid == 0 && v + 1 < NV) {
+				fence_proxy_async_smem();
+				stage_tile(sStream, a.buf.valsIn[v + 1] + tileStart, kTileBytes, &sBar[3]);
+			}
+#pragma unroll
+			for(int i = 0; i < IPT; ++i) sVals[rank[i]] = vals[i];
+			__syncthreads();
+#pragma unroll
+			for(int j = 0; j < IPT; ++j) {
+				const int p = j * NT + tid;
+				if(p < count) {
+					const int dst = sScatter[(sKeys[p] >> shift) & mask] + p;
+					a.buf.valsOut[v][dst] = sVals[p];
+				}
 			}
 		}
+
+		for(int i = tid; i < NW * kDigitBins; i += NT) sWarpHist[i] = 0;
+		__syncthreads();
+
+		// This tile's buffers are free: request the next tile's first value
+		// array, and with one key slot its keys.
+		if(tid == 0 && next < t1 && tile_is_bulk(next)) {
+			fence_proxy_async_smem();
+			if(KSLOTS == 1)
+				stage_tile(sKeys, a.buf.keysIn + (size_t)next * TILE, kTileBytes, &sBar[0]);
+			if constexpr(NV >= 1)
+				stage_tile(sVals, a.buf.valsIn[0] + (size_t)next * TILE, kTileBytes,
+					&sBar[2]);
+		}
+		slot = KSLOTS == 2 ? slot ^ 1 : 0;
 	}
 }
 
@@ -562,43 +690,32 @@ __global__ void iota_kernel(unsigned* out, int n) {
 // Host launchers.
 
 template<int VM>
-static cudaError_t set_pass_attributes() {
-	return cudaFuncSetAttribute(onesweep_kernel<VM>,
-		cudaFuncAttributeMaxDynamicSharedMemorySize,
-		(int)PassLayout<VM>::kBytes);
+static cudaError_t set_sort_attributes() {
+	return cudaFuncSetAttribute(sort_kernel<VM>,
+		cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SortLayout<VM>::kBytes);
 }
 
 cudaError_t configure_kernels() {
 	cudaError_t e = cudaSuccess;
 	cudaError_t r;
-	if((r = set_pass_attributes<-1>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<0>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<1>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<2>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<3>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<4>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<5>()) != cudaSuccess) e = r;
-	if((r = set_pass_attributes<6>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<-1>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<0>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<1>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<2>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<3>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<4>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<5>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<6>()) != cudaSuccess) e = r;
 	return e;
 }
 
 int pass_tile_elements(int valueMode) {
-	switch(valueMode) {
-		case -1: return PassLayout<-1>::TILE;
-		case 0: return PassLayout<0>::TILE;
-		case 1: return PassLayout<1>::TILE;
-		case 2: return PassLayout<2>::TILE;
-		case 3: return PassLayout<3>::TILE;
-		case 4: return PassLayout<4>::TILE;
-		case 5: return PassLayout<5>::TILE;
-		default: return PassLayout<6>::TILE;
-	}
+	(void)valueMode;
+	return kTileElements;
 }
 
-size_t pass_status_bytes(int n, int valueMode) {
-	int tile = pass_tile_elements(valueMode);
-	size_t tiles = n > 0 ? ((size_t)n + tile - 1) / tile : 0;
-	return tiles * kDigitBins * sizeof(unsigned long long);
+size_t pass_scratch_bytes() {
+	return sizeof(unsigned) * kPassScratchWords;
 }
 
 cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
@@ -618,44 +735,115 @@ cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
 	return cudaGetLastError();
 }
 
+// CTAs of the sort kernel that fit on one SM (occupancy), once per mode.
 template<int VM>
-static void launch_pass_vm(const PassArgs& a, cudaStream_t stream) {
-	using L = PassLayout<VM>;
-	onesweep_kernel<VM><<<a.numTiles, L::NT, L::kBytes, stream>>>(a);
+static int sort_ctas_per_sm() {
+	static int perSM = 0;
+	if(!perSM) {
+		int v = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, sort_kernel<VM>,
+			SortLayout<VM>::NT, SortLayout<VM>::kBytes);
+		perSM = v > 0 ? v : 1;
+	}
+	return perSM;
 }
 
-cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
-	int pass, const PassPlan& plan, Control* ctrl,
-	unsigned long long* status, unsigned epoch, bool useBulk, int failTile,
-	volatile unsigned* hostError, cudaStream_t stream) {
-	PassArgs a;
+template<int VM>
+static RangeSplit split_for(int n, int numSMs) {
+	using L = SortLayout<VM>;
+	RangeSplit split;
+	split.numTiles = (int)(((long long)n + L::TILE - 1) / L::TILE);
+	long long ranges = std::min<long long>(split.numTiles,
+		(long long)numSMs * sort_ctas_per_sm<VM>());
+	ranges = std::min<long long>(ranges, kMaxRanges);
+	split.numRanges = (int)std::max<long long>(ranges, 1);
+	split.tilesLo = split.numTiles / split.numRanges;
+	split.extra = split.numTiles % split.numRanges;
+	return split;
+}
+
+static RangeSplit split_for_mode(int valueMode, int n, int numSMs) {
+	switch(valueMode) {
+		case -1: return split_for<-1>(n, numSMs);
+		case 0: return split_for<0>(n, numSMs);
+		case 1: return split_for<1>(n, numSMs);
+		case 2: return split_for<2>(n, numSMs);
+		case 3: return split_for<3>(n, numSMs);
+		case 4: return split_for<4>(n, numSMs);
+		case 5: return split_for<5>(n, numSMs);
+		default: return split_for<6>(n, numSMs);
+	}
+}
+
+cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, unsigned* scratch, int numSMs,
+	cudaStream_t stream) {
+	const RangeSplit split = split_for_mode(valueMode, n, numSMs);
+	unsigned* rangeCounts = scratch;
+	CountArgs c;
+	c.keys = buf.keysIn;
+	c.n = n;
+	c.shift = plan.shift[pass];
+	c.width = plan.width[pass];
+	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
+	c.split = split;
+	c.rangeCounts = rangeCounts;
+	count_kernel<<<split.numRanges, kCountThreads, 0, stream>>>(c);
+
+	ScanArgs s;
+	s.rangeCounts = rangeCounts;
+	s.rangeOffsets = scratch + (size_t)kDigitBins * kMaxRanges;
+	s.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
+	s.numRanges = split.numRanges;
+	scan_kernel<<<kDigitBins / 8, 256, 0, stream>>>(s);
+	return cudaGetLastError();
+}
+
+template<int VM>
+static void launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
+	using L = SortLayout<VM>;
+	sort_kernel<VM><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
+}
+
+cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, Control* ctrl, unsigned* scratch,
+	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream) {
+	SortArgs a;
 	a.buf = buf;
-	a.digitOffsets = ctrl->offsets + plan.binBase[pass];
-	a.trivial = ctrl->trivial + pass;
-	a.tileCounter = ctrl->tileCounter + pass;
-	a.status = status;
+	a.rangeOffsets = scratch + (size_t)kDigitBins * kMaxRanges;
+	a.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
 	a.devError = &ctrl->error;
 	a.hostError = hostError;
+	a.split = split_for_mode(valueMode, n, numSMs);
 	a.n = n;
-	const int tile = pass_tile_elements(valueMode);
-	a.numTiles = (int)(((long long)n + tile - 1) / tile);
 	a.shift = plan.shift[pass];
 	a.width = plan.width[pass];
-	a.epoch = epoch;
 	a.useBulk = useBulk ? 1 : 0;
 	a.failTile = failTile;
 	switch(valueMode) {
-		case -1: launch_pass_vm<-1>(a, stream); break;
-		case 0: launch_pass_vm<0>(a, stream); break;
-		case 1: launch_pass_vm<1>(a, stream); break;
-		case 2: launch_pass_vm<2>(a, stream); break;
-		case 3: launch_pass_vm<3>(a, stream); break;
-		case 4: launch_pass_vm<4>(a, stream); break;
-		case 5: launch_pass_vm<5>(a, stream); break;
-		case 6: launch_pass_vm<6>(a, stream); break;
+		case -1: launch_sort_vm<-1>(a, stream); break;
+		case 0: launch_sort_vm<0>(a, stream); break;
+		case 1: launch_sort_vm<1>(a, stream); break;
+		case 2: launch_sort_vm<2>(a, stream); break;
+		case 3: launch_sort_vm<3>(a, stream); break;
+		case 4: launch_sort_vm<4>(a, stream); break;
+		case 5: launch_sort_vm<5>(a, stream); break;
+		case 6: launch_sort_vm<6>(a, stream); break;
 		default: return cudaErrorInvalidValue;
 	}
 	return cudaGetLastError();
+}
+
+cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, Control* ctrl, unsigned* scratch,
+	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream) {
+	cudaError_t e = launch_pass_count(buf, valueMode, n, pass, plan, scratch,
+		numSMs, stream);
+	if(e != cudaSuccess) return e;
+	return launch_pass_sort(buf, valueMode, n, pass, plan, ctrl, scratch, useBulk,
+		failTile, hostError, numSMs, stream);
 }
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream) {

@@ -53,27 +53,49 @@ struct PassBuffers {
 // value arrays with the keys.
 constexpr int kValueIndex = -1;
 
-// Elements per tile of the pass kernel for a value mode.
+// A pass splits its tiles into at most this many ranges (one CTA each).
+constexpr int kMaxRanges = 1024;
+
+// Device scratch of a pass: per-range digit counts and their exclusive
+// prefixes over ranges (digit-major, [256][kMaxRanges] each) and the digit
+// totals [256]. Reused by every pass; nothing in it needs clearing.
+constexpr size_t kPassScratchWords = 2 * (size_t)kDigitBins * kMaxRanges
+	+ kDigitBins;
+
+// Elements per tile of the sort kernel for a value mode.
 int pass_tile_elements(int valueMode);
 
-// Bytes of lookback status needed for a pass over n elements.
-size_t pass_status_bytes(int n, int valueMode);
+// Bytes of the pass scratch (kPassScratchWords words).
+size_t pass_scratch_bytes();
 
 // Configure kernel attributes (dynamic shared memory); call once per device.
 cudaError_t configure_kernels();
 
+// Digit histograms of every pass of `plan` in one read of the keys, their
+// exclusive scans and the per-pass "single digit" flags (earlyExit).
 cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
 	Control* ctrl, volatile unsigned* hostError, int numSMs,
 	cudaStream_t stream);
 
+// One pass (count, scan and sort kernels) by the digit of plan pass `pass`.
 // useBulk: every buffer of the pass is 16-byte aligned, so full tiles are
 // staged with bulk copies; otherwise every tile uses plain loads.
-// failTile >= 0 makes that tile skip its lookback publication (fault
-// injection for tests of the bounded waits); -1 in normal use.
+// failTile >= 0 makes the CTA that sorts that tile run a bounded wait out
+// (fault injection for tests); -1 in normal use.
 cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
-	int pass, const PassPlan& plan, Control* ctrl,
-	unsigned long long* status, unsigned epoch, bool useBulk, int failTile,
-	volatile unsigned* hostError, cudaStream_t stream);
+	int pass, const PassPlan& plan, Control* ctrl, unsigned* scratch,
+	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream);
+
+// The two halves of launch_pass: the count and scan kernels, then the sort
+// kernel (the engine times them separately).
+cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, unsigned* scratch, int numSMs,
+	cudaStream_t stream);
+cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
+	int pass, const PassPlan& plan, Control* ctrl, unsigned* scratch,
+	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream);
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream);
 

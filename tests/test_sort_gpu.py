@@ -293,7 +293,7 @@ def test_async_stream(engine, oracle_mod):
 
 
 def test_bounded_wait_reports_kernel_error(engine, oracle_mod):
-    """A tile that never publishes makes the later tiles' lookback waits run
+    """A CTA that waits on a barrier nothing completes runs its bounded wait
     out: the sort reports KERNEL_ERROR (no fault, no hang) and the engine
     keeps working."""
     from mgpu_old_b200 import api
