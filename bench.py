@@ -118,11 +118,68 @@ def cpu_baseline(case, budget_s=10.0):
                       f"{total_n // sample_n} repetitions"}
 
 
+def cpu_baseline_segmented(case, budget_s=10.0):
+    """The oracle's per-segment stable sort on a bounded sample of segments."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    sizes = np.diff(case.offsets.astype(np.int64))
+    take = int(np.searchsorted(np.cumsum(sizes), CPU_SAMPLE)) + 1
+    take = max(1, min(take, case.num_segments))
+    end = int(case.offsets[take])
+    offs = case.offsets[:take + 1]
+    keys = case.keys[:end]
+    vals = [case.values[0][:end]]
+    total_t, total_n = 0.0, 0
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or total_n == 0:
+        t0 = time.perf_counter()
+        oracle.sort_segments(keys, vals, 1, offs, case.first_bit, case.end_bit)
+        total_t += time.perf_counter() - t0
+        total_n += end
+    return {"value": round(total_n / total_t / 1e6, 3), "unit": UNIT, "cores": 1,
+            "kind": "port",
+            "sample": f"first {take} segments ({end} elements) of {case.name}, oracle "
+                      f"std::stable_sort per segment, 1 thread, {total_n // end} repetitions"}
+
+
+def run_reference_segmented(args, case):
+    """Reference arm for a segmented workload: the oracle's per-segment
+    stable sort (what a per-segment loop of the CPU path computes) over a
+    bounded sample of segments per step."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    sizes = np.diff(case.offsets.astype(np.int64))
+    take = max(1, min(case.num_segments, int(np.searchsorted(np.cumsum(sizes), CPU_SAMPLE)) + 1))
+    end = int(case.offsets[take])
+    offs, keys, vals = case.offsets[:take + 1], case.keys[:end], [case.values[0][:end]]
+    for _ in range(args.warmup):
+        oracle.sort_segments(keys, vals, 1, offs, case.first_bit, case.end_bit)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.sort_segments(keys, vals, 1, offs, case.first_bit, case.end_bit)
+        times.append(time.perf_counter() - t0)
+    value = end * len(times) / sum(times) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(sum(times) / len(times) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": workload_config(case, args, {"sample_segments": take, "sample": end}),
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"first {take} segments per step"},
+            "e2e": {"value": round(value, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     case = workloads.WORKLOADS[args.workload]()
+    if isinstance(case, workloads.SegmentedCase):
+        return run_reference_segmented(args, case)
     threads = os.cpu_count() or 1
     sample_n = min(case.n, CPU_SAMPLE)
     for _ in range(args.warmup):
@@ -285,6 +342,178 @@ def verify(case, keys, vals):
         assert (idx[1:][eq] > idx[:-1][eq]).all(), "not stable"
 
 
+def run_segmented(args, case, device, barrier, max_over_ranks, world, rank, local):
+    """Batched segmented sort (sortSegmentedArray) against a loop of plain
+    sortArray calls, one per segment, on the same GPU."""
+    import torch
+    from mgpu_old_b200 import api
+
+    sorter = GpuSorter(case, device)
+    offs_t = torch.from_numpy(case.offsets.astype(np.int32)).to(device)
+    engine = api.MgpuSort()
+    d = sorter.data
+    S = case.num_segments
+    stream = torch.cuda.current_stream(device)
+
+    def one_sort():
+        api.check(engine.sort_segmented(d, offs_t.data_ptr(), S))
+
+    for _ in range(max(args.warmup, 3)):
+        sorter.restore()
+        sorter.flush_l2()
+        one_sort()
+    api.check(engine.synchronize())
+    torch.cuda.synchronize()
+
+    engine.enable_kernel_timing(True)
+    engine.read_kernel_timing()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        sorter.restore()
+        sorter.flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_sort()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    barrier()
+    clk = clocks.stop()
+    kt = engine.read_kernel_timing()
+    engine.enable_kernel_timing(False)
+    api.check(engine.synchronize())
+    keys, vals = sorter.result()
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+    value = case.n * world / (ms_per_step * 1e-3) / 1e6
+
+    # The per-call baseline: every segment in its own 16-byte aligned buffers,
+    # one sortArray call each, timed over whole loops.
+    sizes = np.diff(case.offsets.astype(np.int64))
+    padded = (sizes + 3) // 4 * 4
+    poff = np.zeros(S + 1, np.int64)
+    np.cumsum(padded, out=poff[1:])
+    total = int(poff[-1]) + 2048
+    src_k = np.zeros(total, np.uint32)
+    src_v = np.zeros(total, np.uint32)
+    for i in range(S):
+        a, b = int(case.offsets[i]), int(case.offsets[i + 1])
+        src_k[poff[i]:poff[i] + (b - a)] = case.keys[a:b]
+        src_v[poff[i]:poff[i] + (b - a)] = case.values[0][a:b]
+    pk = torch.from_numpy(src_k.view(np.int32)).to(device)
+    pv = torch.from_numpy(src_v.view(np.int32)).to(device)
+    k0, k1 = pk.clone(), torch.empty_like(pk)
+    v0, v1 = pv.clone(), torch.empty_like(pv)
+    datas = []
+    for i in range(S):
+        sd = api.SortData()
+        sd.maxElements = sd.numElements = int(sizes[i])
+        sd.valueCount = 1
+        sd.firstBit, sd.endBit = case.first_bit, case.end_bit
+        off = 4 * int(poff[i])
+        sd.keys[0], sd.keys[1] = k0.data_ptr() + off, k1.data_ptr() + off
+        sd.values[0][0], sd.values[0][1] = v0.data_ptr() + off, v1.data_ptr() + off
+        datas.append(sd)
+    lib = api.load_library()
+    h = engine.handle
+    loop_steps = max(1, min(2, args.steps))
+    loop_ms = 0.0
+    for step in range(loop_steps + 1):
+        k0.copy_(pk)
+        v0.copy_(pv)
+        sorter.flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for sd in datas:
+            api.check(lib.sortArray(h, ctypes_byref(sd)))
+        e1.record(stream)
+        e1.synchronize()
+        if step > 0:                       # the first loop is a warm-up
+            loop_ms += e0.elapsed_time(e1)
+    api.check(engine.synchronize())
+    loop_ms /= loop_steps
+    lk = k0.cpu().numpy().view(np.uint32)
+    lv = v0.cpu().numpy().view(np.uint32)
+    same = True
+    for i in range(S):
+        a, b = int(case.offsets[i]), int(case.offsets[i + 1])
+        p0 = int(poff[i])
+        same &= np.array_equal(keys[a:b], lk[p0:p0 + (b - a)])
+        same &= np.array_equal(vals[0][a:b], lv[p0:p0 + (b - a)])
+    if not same:
+        raise AssertionError("batched result differs from the per-call sortArray loop")
+
+    # End to end through the C ABI with pinned host buffers.
+    pin_k = torch.from_numpy(case.keys.view(np.int32)).pin_memory()
+    pin_v = torch.from_numpy(case.values[0].view(np.int32)).pin_memory()
+    pin_o = torch.from_numpy(case.offsets.astype(np.int32)).pin_memory()
+    out_k = torch.empty(case.n, dtype=torch.int32).pin_memory()
+    out_v = torch.empty(case.n, dtype=torch.int32).pin_memory()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        sorter.flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sorter.bufs[d.keys[0]][:case.n].copy_(pin_k, non_blocking=True)
+        sorter.bufs[d.values[0][0]][:case.n].copy_(pin_v, non_blocking=True)
+        offs_t.copy_(pin_o, non_blocking=True)
+        one_sort()
+        out_k.copy_(sorter.bufs[d.keys[0]][:case.n], non_blocking=True)
+        out_v.copy_(sorter.bufs[d.values[0][0]][:case.n], non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    api.check(engine.synchronize())
+    e2e_ms = max_over_ranks(e2e_ms)
+    e2e_value = case.n * world / (e2e_ms / args.steps * 1e-3) / 1e6
+
+    peak, peak_src = hbm_peak()
+    large = sizes[sizes > 4096].sum()
+    passes = len(_plan(case))
+    pass_bytes = 2 * int(large) * 4 * 2
+    pass_ms = kt["pass_ms"] / max(kt["pass_launches"], 1)
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    alg = workloads.algorithmic_bytes(case.n, case.first_bit, case.end_bit, case.value_count)
+    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded numpy)",
+            "config": workload_config(case, args, {"segments": S,
+                                                  "large_segment_elements": int(large)}),
+            "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * case.n + 4 * (S + 1),
+                    "d2h_bytes_per_step": 8 * case.n},
+            "per_call_loop": {"ms_per_step": round(loop_ms, 3),
+                              "Mkeys_s": round(case.n / (loop_ms * 1e-3) / 1e6, 1),
+                              "speedup": round(loop_ms / ms_per_step, 2),
+                              "identical_output": True},
+            "gpu_launches": 2 + 2 * kt["upsweep_launches"] + 3 * kt["pass_launches"],
+            "roofline": {"bound": "hbm", "kernel": "seg pass (count+scan+sort)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                         "traffic": None, "bytes_per_launch": pass_bytes,
+                         "avg_launch_ms": round(pass_ms, 5),
+                         "whole_sort": {"alg_bytes": alg,
+                                        "achieved": round(alg / (ms_per_step * 1e-3) / 1e9, 1),
+                                        "frac": round(alg / (ms_per_step * 1e-3) / 1e9 / peak, 4)},
+                         "small_segments_avg_ms": round(
+                             kt["upsweep_ms"] / max(kt["upsweep_launches"], 1), 5)},
+            "clocks": clk}
+    engine.release()
+    return line
+
+
+def ctypes_byref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -317,6 +546,16 @@ def main():
     from mgpu_old_b200 import api
     api.load_library()
     case = workloads.WORKLOADS[args.workload]()
+    if isinstance(case, workloads.SegmentedCase):
+        line = run_segmented(args, case, device, barrier, max_over_ranks, world, rank, local)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_segmented(case)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line))
+        return 0
     sorter = GpuSorter(case, device)
     engine = api.MgpuSort()
     d = sorter.data

@@ -32,7 +32,7 @@ int SORTAPI sortPlanPasses(int firstBit, int endBit, int bitPass,
 	int* widths);
 
 /* Fault injection for tests of the device-side bounded waits: in the next
- * pass launched by this engine, the CTA that sorts tile `tile` (4096
+ * pass launched by this engine, the CTA that sorts tile `tile` (7680 or 7168
  * elements each) also waits on a barrier that nothing completes, so that
  * bounded wait runs out (about half a second) and the sort reports
  * SORT_STATUS_KERNEL_ERROR through sortSynchronize. -1 turns it off. Nothing
@@ -49,6 +49,21 @@ sortStatus_t SORTAPI sortInjectFault(sortEngine_t engine, int tile);
 sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable);
 sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches);
+
+/* Batched segmented sort: sort each of numSegments independent segments of
+ * the array described by `data` stably by its bit field, in one call. No
+ * counterpart in the reference, whose callers sort many arrays with one
+ * sortArray call each. segmentOffsets is a DEVICE array of numSegments + 1
+ * ints: segment i is [segmentOffsets[i], segmentOffsets[i + 1]), with
+ * segmentOffsets[0] == 0, non-decreasing, segmentOffsets[numSegments] ==
+ * data->numElements (otherwise SORT_STATUS_KERNEL_ERROR is reported, by
+ * sortSynchronize, and nothing is sorted). Buffers, value modes, swaps and
+ * parity are sortArray's; every segment goes through the same passes, and
+ * index mode writes positions within the segment. earlyExit is ignored.
+ * Runs on `stream` (0: the legacy default stream); one engine runs one sort
+ * at a time. The result equals one sortArray per segment. */
+sortStatus_t SORTAPI sortSegmentedArray(sortEngine_t engine, sortData_t data,
+	const int* segmentOffsets, int numSegments, CUstream stream);
 
 /* Largest numElements that sortArrayNoAlloc accepts (4 Mi elements). */
 #define SORT_NOALLOC_MAX_ELEMENTS 4194304

@@ -66,6 +66,7 @@ EXPORTED_SYMBOLS = (
     # mgpusort_b200.h (no reference counterpart)
     "sortArrayAsync", "sortSynchronize", "sortPlanPasses", "sortInjectFault",
     "sortEnableKernelTiming", "sortReadKernelTiming", "sortArrayNoAlloc",
+    "sortSegmentedArray",
 )
 
 # Largest numElements accepted by sortArrayNoAlloc (SORT_NOALLOC_MAX_ELEMENTS).
@@ -107,6 +108,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "sortReadKernelTiming": (c_int, [engine_t, POINTER(ctypes.c_double), POINTER(c_int),
                                          POINTER(ctypes.c_double), POINTER(c_int)]),
         "sortArrayNoAlloc": (c_int, [data_t, c_void_p]),
+        "sortSegmentedArray": (c_int, [engine_t, data_t, c_void_p, c_int, c_void_p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -183,6 +185,14 @@ class MgpuSort:
 
     def synchronize(self) -> int:
         return load_library().sortSynchronize(self._engine)
+
+    def sort_segmented(self, data: SortData, offsets_ptr: int, num_segments: int,
+                       stream: int = 0) -> int:
+        """sortSegmentedArray: offsets_ptr is a device int array of
+        num_segments + 1 segment boundaries."""
+        return load_library().sortSegmentedArray(self._engine, ctypes.byref(data),
+                                                 c_void_p(offsets_ptr), num_segments,
+                                                 c_void_p(stream))
 
     def enable_kernel_timing(self, enable: bool = True) -> None:
         check(load_library().sortEnableKernelTiming(self._engine, int(enable)))

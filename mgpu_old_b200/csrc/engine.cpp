@@ -74,6 +74,9 @@ struct sortEngine_d {
 	mgpusort::Control* ctrl = nullptr;
 	// Per-pass scratch: range digit counts, their prefixes, digit totals.
 	unsigned* scratch = nullptr;
+	// Segmented-sort scratch, grown on demand.
+	void* segScratch = nullptr;
+	size_t segScratchBytes = 0;
 	// Host-mapped error word written by kernels, read without synchronizing.
 	volatile unsigned* hostError = nullptr;
 	unsigned* hostErrorDev = nullptr;
@@ -125,6 +128,7 @@ void destroy_engine(sortEngine_d* e) {
 	}
 	if(e->ctrl) cudaFree(e->ctrl);
 	if(e->scratch) cudaFree(e->scratch);
+	if(e->segScratch) cudaFree(e->segScratch);
 	if(e->hostError) cudaFreeHost(const_cast<unsigned*>(e->hostError));
 	if(e->hostTrivial) cudaFreeHost(e->hostTrivial);
 	if(e->done) cudaEventDestroy(e->done);
@@ -287,6 +291,104 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 		ce = mgpusort::launch_iota(reinterpret_cast<unsigned*>(d->values1[0]), n,
 			stream);
 		if(ce != cudaSuccess) return launch_status(ce);
+	}
+	cudaEventRecord(e->done, stream);
+	return SORT_STATUS_SUCCESS;
+}
+
+// Checks shared by the sort entry points: bit range, sizes, value mode and
+// buffers. Returns SUCCESS with *work = false when there is nothing to do.
+sortStatus_t validate(const sortData_d* d, bool* work) {
+	*work = false;
+	const int numBits = d->endBit - d->firstBit;
+	if(!numBits) return SORT_STATUS_SUCCESS;
+	if(numBits < 0 || numBits > 32 || d->firstBit < 0 || d->endBit > 32)
+		return SORT_STATUS_INVALID_VALUE;
+	if(d->numElements > d->maxElements || d->numElements < 0)
+		return SORT_STATUS_INVALID_VALUE;
+	if(d->valueCount < -1 || d->valueCount > 6) return SORT_STATUS_INVALID_VALUE;
+	const int numArrays = d->valueCount == -1 ? 1 : d->valueCount;
+	if(!d->keys[0] || !d->keys[1]) return SORT_STATUS_INVALID_VALUE;
+	for(int i = 0; i < numArrays; ++i)
+		if(!d->values[i][0] || !d->values[i][1]) return SORT_STATUS_INVALID_VALUE;
+	*work = d->numElements > 0;
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
+	int numSegments, cudaStream_t stream) {
+	if(!e || !d || !offsets || numSegments < 1) return SORT_STATUS_INVALID_VALUE;
+	sortStatus_t pending = take_device_error(e);
+	if(pending != SORT_STATUS_SUCCESS) return pending;
+	bool work = false;
+	sortStatus_t st = validate(d, &work);
+	if(st != SORT_STATUS_SUCCESS || !work) return st;
+	const int n = d->numElements;
+	const bool indexMode = d->valueCount == -1;
+	const int numArrays = indexMode ? 1 : d->valueCount;
+
+	mgpusort::PassPlan plan;
+	if(!make_plan(d->firstBit, d->endBit - d->firstBit, 0, &plan))
+		return SORT_STATUS_INTERNAL_ERROR;
+
+	const size_t bytes = mgpusort::seg_scratch_bytes(n, numSegments);
+	if(bytes > e->segScratchBytes) {
+		if(e->segScratch) cudaFree(e->segScratch);
+		e->segScratch = nullptr;
+		e->segScratchBytes = 0;
+		if(cudaMalloc(&e->segScratch, bytes) != cudaSuccess) {
+			cudaGetLastError();
+			e->segScratch = nullptr;
+			return SORT_STATUS_DEVICE_ALLOC_FAILED;
+		}
+		e->segScratchBytes = bytes;
+	}
+	if(e->dirty) {
+		if(cudaMemsetAsync(e->ctrl, 0, sizeof(mgpusort::Control), stream)
+			!= cudaSuccess) return SORT_STATUS_DEVICE_ERROR;
+		e->dirty = false;
+	}
+	bool bulk = true;
+	for(int i = 0; i < 2; ++i) bulk = bulk && aligned16(d->keys[i]);
+	for(int i = 0; i < numArrays; ++i)
+		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
+
+	const int firstMode = indexMode ? mgpusort::kValueIndex : numArrays;
+	cudaError_t ce = mgpusort::launch_seg_plan(offsets, numSegments, n, firstMode,
+		e->segScratch, e->ctrl, e->hostErrorDev, stream);
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+
+	// Segments of up to 4096 elements: every pass in shared memory, straight
+	// into the buffers that hold the result after all passes' swaps.
+	const int last = plan.numPasses & 1;
+	mgpusort::PassBuffers small = {};
+	small.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
+	small.keysOut = reinterpret_cast<unsigned*>(d->keys[last]);
+	for(int i = 0; i < 6; ++i) {
+		small.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
+		small.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][last]);
+	}
+	int slot = timing_begin(e, kTimedUpsweep, stream);
+	ce = mgpusort::launch_seg_small(small, firstMode, plan, offsets, numSegments, n,
+		e->segScratch, e->numSMs, stream);
+	timing_end(e, slot, stream);
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+
+	for(int p = 0; p < plan.numPasses; ++p) {
+		const int vm = (indexMode && p == 0) ? mgpusort::kValueIndex : numArrays;
+		mgpusort::PassBuffers buf = {};
+		buf.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
+		buf.keysOut = reinterpret_cast<unsigned*>(d->keys[1]);
+		for(int i = 0; i < 6; ++i) {
+			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
+			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
+		}
+		slot = timing_begin(e, kTimedPass, stream);
+		ce = mgpusort::launch_seg_pass(buf, vm, p, plan, offsets, numSegments, n,
+			e->segScratch, e->ctrl, bulk, e->hostErrorDev, e->numSMs, stream);
+		timing_end(e, slot, stream);
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+		swap_buffers(d);
 	}
 	cudaEventRecord(e->done, stream);
 	return SORT_STATUS_SUCCESS;
@@ -480,6 +582,12 @@ sortStatus_t SORTAPI sortArrayEx(sortEngine_t engine, sortData_t data,
 sortStatus_t SORTAPI sortArrayAsync(sortEngine_t engine, sortData_t data,
 	CUstream stream) {
 	return sort_impl(engine, data, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+sortStatus_t SORTAPI sortSegmentedArray(sortEngine_t engine, sortData_t data,
+	const int* segmentOffsets, int numSegments, CUstream stream) {
+	return segmented_impl(engine, data, segmentOffsets, numSegments,
+		stream ? reinterpret_cast<cudaStream_t>(stream) : cudaStreamLegacy);
 }
 
 sortStatus_t SORTAPI sortSynchronize(sortEngine_t engine) {

@@ -13,6 +13,7 @@ constexpr unsigned kErrLookbackTimeout = 1u;
 constexpr unsigned kErrBarrierTimeout = 2u;
 constexpr unsigned kErrQueueTimeout = 4u;
 constexpr unsigned kErrInjected = 8u;
+constexpr unsigned kErrBadSegments = 16u;
 
 // Bounded waits. A poll of a status word or an mbarrier normally succeeds
 // within microseconds. After kSpinFastPolls polls a waiter backs off with

@@ -193,12 +193,12 @@ struct RangeSplit {
 	}
 };
 
-constexpr int kTileElements = 4096;
 constexpr int kCountThreads = 512;
 
 struct CountArgs {
 	const unsigned* keys;
 	int n;
+	int tile;                       // elements per tile of the sort kernel
 	int shift;
 	int width;
 	int vecOk;
@@ -206,26 +206,29 @@ struct CountArgs {
 	unsigned* rangeCounts;          // [256][R], digit-major
 };
 
+// Each lane owns one copy of the histogram, interleaved so that bin b of
+// lane l is word b * 32 + l: every atomic of a warp falls in its own bank,
+// and lanes never share a counter (warps do, through the atomic).
 __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a) {
-	__shared__ unsigned sHist[kDigitBins * kUpCopies];
+	__shared__ unsigned sHist[kDigitBins * 32];
 	const int tid = threadIdx.x;
-	const int copy = tid & (kUpCopies - 1);
+	const int lane = tid & 31;
 	const int r = blockIdx.x;
 	const unsigned mask = (1u << a.width) - 1;
 	const int shift = a.shift;
 
-	for(int i = tid; i < kDigitBins * kUpCopies; i += kCountThreads) sHist[i] = 0;
+	for(int i = tid; i < kDigitBins * 32; i += kCountThreads) sHist[i] = 0;
 	__syncthreads();
 
-	const long long begin = (long long)a.split.first_tile(r) * kTileElements;
+	const long long begin = (long long)a.split.first_tile(r) * a.tile;
 	const long long end = min((long long)a.n,
-		(long long)a.split.first_tile(r + 1) * kTileElements);
-	auto add = [&](unsigned k) {
-		atomicAdd(&sHist[((k >> shift) & mask) * kUpCopies + copy], 1u);
-	};
+		(long long)a.split.first_tile(r + 1) * a.tile);
+	unsigned* myCol = sHist + lane;
+	auto add = [&](unsigned k) { atomicAdd(&myCol[((k >> shift) & mask) * 32], 1u); };
 	long long done = begin;
 	if(a.vecOk) {
-		// begin is a multiple of the tile size: 16-byte aligned.
+		// begin is a multiple of the tile size (a multiple of 4): 16-byte
+		// aligned.
 		const uint4* src = reinterpret_cast<const uint4*>(a.keys + begin);
 		const int nvec = (int)((end - begin) / 4);
 		constexpr int U = 4;
@@ -254,11 +257,13 @@ __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a)
 	for(long long e = done + tid; e < end; e += kCountThreads) add(a.keys[e]);
 	__syncthreads();
 
-	if(tid < kDigitBins) {
-		unsigned c = 0;
+	// Sum the 32 copies of each bin: warp w sums bins w, w + 16, ...; lane l
+	// reads copy l of the bin, a warp reduction adds them up.
+	for(int b = tid >> 5; b < kDigitBins; b += kCountThreads / 32) {
+		unsigned c = sHist[b * 32 + lane];
 #pragma unroll
-		for(int j = 0; j < kUpCopies; ++j) c += sHist[tid * kUpCopies + j];
-		a.rangeCounts[(size_t)tid * a.split.numRanges + r] = c;
+		for(int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+		if(lane == 0) a.rangeCounts[(size_t)b * a.split.numRanges + r] = c;
 	}
 }
 
@@ -300,10 +305,15 @@ struct SortArgs {
 	int failTile;                   // tile whose CTA runs a wait out; -1: none
 };
 
+// Tile shapes measured on B200 (sort kernel time over 32 Mi and 64 Mi
+// key-value pairs and 16 Mi keys with six value arrays, 256..512 threads x
+// 12..32 keys): larger tiles give each digit longer runs per tile, so fewer
+// partially written sectors reach DRAM; 384 x 20 was best for keys, indices
+// and one value array, 512 x 14 for several value arrays.
 template<int VM> struct SortConfig {
-	static constexpr int kThreads = 256;
-	static constexpr int kItems = 16;
-	static constexpr int kMinBlocks = 3;
+	static constexpr int kThreads = VM >= 2 ? 512 : 384;
+	static constexpr int kItems = VM >= 2 ? 14 : 20;
+	static constexpr int kMinBlocks = 2;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
@@ -335,7 +345,7 @@ template<int VM> struct SortLayout {
 	static constexpr int kWords = kBar + 2 * 6;       // 6 mbarriers
 	static constexpr size_t kBytes = sizeof(unsigned) * kWords;
 	static_assert(kBar % 2 == 0, "mbarriers need 8-byte alignment");
-	static_assert(TILE == kTileElements, "count and sort kernels share tiles");
+	static_assert(TILE < 65536, "ranks are packed in 16 bits");
 };
 
 // Peers of an 8-bit digit: the lanes of the warp whose digit equals this
@@ -360,17 +370,16 @@ __device__ __forceinline__ unsigned match_digit8(unsigned d,
 	return __shfl_sync(0xffffffffu, lo, d & 15u) & __shfl_sync(0xffffffffu, hi, d >> 4);
 }
 
-// Stable warp rank of one item: the highest peer adds the group's size to
-// the warp's running count of the digit; the old count, broadcast, is the
-// group's base. Returns (digit << 16) | rank within the warp.
+// Stable warp rank of one item: the group of peers starts at the warp's
+// running count of the digit, which the highest peer then advances by the
+// group's size. Returns (digit << 16) | rank within the warp.
 __device__ __forceinline__ unsigned rank_item(unsigned d, unsigned* warpHist,
 	int lane, unsigned ltMask, const unsigned (&nClear)[4]) {
 	const unsigned peers = match_digit8(d, nClear);
-	const int leader = 31 - __clz(peers);
-	unsigned base = 0;
-	if(lane == leader) base = atomicAdd(&warpHist[d], (unsigned)__popc(peers));
-	base = __shfl_sync(0xffffffffu, base, leader);
-	// Orders this item's counter update before the next item's.
+	// Every peer reads the count; the highest peer then adds the group.
+	const unsigned base = warpHist[d];
+	__syncwarp();
+	if((peers >> lane) == 1u) warpHist[d] = base + __popc(peers);
 	__syncwarp();
 	return (d << 16) | (base + __popc(peers & ltMask));
 }
@@ -381,26 +390,95 @@ __device__ __forceinline__ void stage_tile(unsigned* dst, const unsigned* src,
 	bulk_load(dst, src, bytes, bar);
 }
 
+// The digit of a key. A whole byte (8-bit digit at a multiple of 8) is one
+// byte permute; any other field a shift and a mask.
+template<bool BYTE> struct DigitOf {
+	int shift;
+	unsigned mask;
+	unsigned sel;
+	__device__ __forceinline__ DigitOf(int s, int width)
+		: shift(s), mask((1u << width) - 1), sel(0x4440u | (unsigned)(s >> 3)) { }
+	__device__ __forceinline__ unsigned operator()(unsigned k) const {
+		if constexpr(BYTE) return __byte_perm(k, 0u, sel);
+		else return (k >> shift) & mask;
+	}
+};
+
 // Rank the staged tile's keys (warp-striped: item i of lane l in warp w is
 // tile element w*32*IPT + i*32 + l, so (item, lane) order is input order per
 // warp). In a partial tile the elements past `count` get digit 255: they
 // rank after every real key and are never stored.
-template<int IPT, bool FULL>
+template<int IPT, bool FULL, bool BYTE>
 __device__ __forceinline__ void rank_tile(const unsigned* sKeys, unsigned* myHist,
-	int warpBase, int lane, int count, int shift, unsigned mask, unsigned ltMask,
+	int warpBase, int lane, int count, const DigitOf<BYTE>& digit, unsigned ltMask,
 	const unsigned (&nClear)[4], unsigned (&rank)[IPT]) {
 #pragma unroll
 	for(int i = 0; i < IPT; ++i) {
 		const int idx = warpBase + i * 32 + lane;
-		unsigned d = (sKeys[idx] >> shift) & mask;
+		unsigned d = digit(sKeys[idx]);
 		if(!FULL && idx >= count) d = kDigitBins - 1;
 		rank[i] = rank_item(d, myHist, lane, ltMask, nClear);
 	}
 }
 
+// Shared-memory arrays of the sort kernels.
+template<int VM> struct SortSmem {
+	using L = SortLayout<VM>;
+	unsigned* smem;
+	unsigned* vals;
+	unsigned* stream;
+	unsigned* warpHist;
+	unsigned* running;
+	int* scatter;
+	unsigned* scan;
+	// mbarriers: [0..1] key slots, [2] value buffer, [3] stream buffer,
+	// [5] injected-fault wait (never completed).
+	uint64_t* bar;
+	__device__ __forceinline__ explicit SortSmem(unsigned* base)
+		: smem(base), vals(base + L::kVals), stream(base + L::kStream),
+		  warpHist(base + L::kWarpHist), running(base + L::kRunning),
+		  scatter(reinterpret_cast<int*>(base + L::kScatter)), scan(base + L::kScan),
+		  bar(reinterpret_cast<uint64_t*>(base + L::kBar)) { }
+	__device__ __forceinline__ unsigned* keys(int slot) const {
+		return smem + L::kKeys + slot * L::TILE;
+	}
+};
+
+// Once per CTA: mbarriers and zeroed warp histograms.
 template<int VM>
-__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
-sort_kernel(const SortArgs a) {
+__device__ __forceinline__ void sort_setup(const SortSmem<VM>& sm) {
+	using L = SortLayout<VM>;
+	if(threadIdx.x == 0) {
+		for(int i = 0; i < 6; ++i) mbar_init(&sm.bar[i], 1);
+		fence_mbar_init();
+	}
+	for(int i = threadIdx.x; i < L::NW * kDigitBins; i += L::NT) sm.warpHist[i] = 0;
+}
+
+// Identity pass over [begin, end) (every key has the same digit).
+template<int VM>
+__device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
+	long long end, long long indexBase) {
+	constexpr int NV = SortLayout<VM>::NV;
+	for(long long i = begin + threadIdx.x; i < end; i += SortLayout<VM>::NT) {
+		a.buf.keysOut[i] = a.buf.keysIn[i];
+		if constexpr(VM == kValueIndex) a.buf.valsOut[0][i] = (unsigned)(i - indexBase);
+#pragma unroll
+		for(int v = 0; v < NV; ++v) a.buf.valsOut[v][i] = a.buf.valsIn[v][i];
+	}
+}
+
+// Sort the tiles of [begin, end) in order, from digit offsets already in
+// sm.running (element p of digit d's run in a tile goes to running[d] + p,
+// then running[d] advances by the tile's count). Each tile: stable warp
+// ranks, digit starts, reorder into digit runs in shared memory, run-wise
+// stores; value arrays past the first stream through one buffer. The next
+// tile's keys are copied in while a tile is sorted (two key slots), its
+// first value array as soon as this tile has stored its own. Index mode
+// writes position - indexBase. Requires sort_setup and a barrier before.
+template<int VM, bool BYTE>
+__device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
+	long long begin, long long end, long long indexBase, unsigned& phase) {
 
 	using L = SortLayout<VM>;
 	constexpr int NT = L::NT;
@@ -411,90 +489,48 @@ sort_kernel(const SortArgs a) {
 	constexpr int KSLOTS = L::KSLOTS;
 	constexpr unsigned kTileBytes = TILE * 4;
 
-	extern __shared__ __align__(128) unsigned smem[];
-	unsigned* sVals = smem + L::kVals;
-	unsigned* sStream = smem + L::kStream;
-	unsigned* sWarpHist = smem + L::kWarpHist;
-	unsigned* sRunning = smem + L::kRunning;
-	int* sScatter = reinterpret_cast<int*>(smem + L::kScatter);
-	unsigned* sScan = smem + L::kScan;
-	// mbarriers: [0..1] key slots, [2] value buffer, [3] stream buffer,
-	// [5] injected-fault wait (never completed).
-	uint64_t* sBar = reinterpret_cast<uint64_t*>(smem + L::kBar);
+	unsigned* sVals = sm.vals;
+	unsigned* sStream = sm.stream;
+	unsigned* sWarpHist = sm.warpHist;
+	unsigned* sRunning = sm.running;
+	int* sScatter = sm.scatter;
+	unsigned* sScan = sm.scan;
+	uint64_t* sBar = sm.bar;
 
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
 	const int warpBase = warp * 32 * IPT;
-	const int r = blockIdx.x;
-	const int t0 = a.split.first_tile(r);
-	const int t1 = a.split.first_tile(r + 1);
-	const int R = a.split.numRanges;
 
-	// Each digit starts at the keys with smaller digits in the whole array
-	// plus the keys with this digit in the ranges before this one.
-	const unsigned total = tid < kDigitBins ? a.totals[tid] : 0u;
-	const unsigned inclTotal = warp_inclusive_scan(total, lane);
-	if(lane == 31 && tid < kDigitBins) sScan[warp] = inclTotal;
-	const int nonEmpty = __syncthreads_count(tid < kDigitBins && total != 0);
-	if(tid < kDigitBins) {
-		unsigned prefix = 0;
-		for(int w = 0; w < warp; ++w) prefix += sScan[w];
-		sRunning[tid] = prefix + inclTotal - total + a.rangeOffsets[(size_t)tid * R + r];
-	}
-
-	if(nonEmpty <= 1) {
-		// Every key has the same digit: the pass is the identity.
-		const long long b = (long long)t0 * TILE;
-		const long long e = min((long long)a.n, (long long)t1 * TILE);
-		for(long long i = b + tid; i < e; i += NT) {
-			a.buf.keysOut[i] = a.buf.keysIn[i];
-			if constexpr(VM == kValueIndex) a.buf.valsOut[0][i] = (unsigned)i;
-#pragma unroll
-			for(int v = 0; v < NV; ++v) a.buf.valsOut[v][i] = a.buf.valsIn[v][i];
-		}
-		return;
-	}
-
-	auto tile_is_bulk = [&](int t) {
-		return a.useBulk && (long long)(t + 1) * TILE <= a.n;
+	// Full tiles at 16-byte aligned offsets are staged with bulk copies.
+	auto tile_is_bulk = [&](long long t) {
+		return a.useBulk && (t & 3) == 0 && t + TILE <= end;
 	};
 
-	if(tid == 0) {
-		for(int i = 0; i < 6; ++i) mbar_init(&sBar[i], 1);
-		fence_mbar_init();
-		if(t0 < t1 && tile_is_bulk(t0)) {
-			stage_tile(smem + L::kKeys, a.buf.keysIn + (size_t)t0 * TILE, kTileBytes,
-				&sBar[0]);
-			if constexpr(NV >= 1)
-				stage_tile(sVals, a.buf.valsIn[0] + (size_t)t0 * TILE, kTileBytes, &sBar[2]);
-		}
+	if(tid == 0 && begin < end && tile_is_bulk(begin)) {
+		fence_proxy_async_smem();
+		stage_tile(sm.keys(0), a.buf.keysIn + begin, kTileBytes, &sBar[0]);
+		if constexpr(NV >= 1) stage_tile(sVals, a.buf.valsIn[0] + begin, kTileBytes, &sBar[2]);
 	}
-	for(int i = tid; i < NW * kDigitBins; i += NT) sWarpHist[i] = 0;
-	__syncthreads();
 
-	const unsigned mask = (1u << a.width) - 1;
-	const int shift = a.shift;
+	const DigitOf<BYTE> digit(a.shift, a.width);
 	const unsigned ltMask = lanemask_lt();
 	unsigned nClear[4];
 #pragma unroll
 	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
-	unsigned phase = 0;    // bit s: key slot s; bit 2: value buffer; bit 3: stream
 	int slot = 0;
 
-	for(int tile = t0; tile < t1; ++tile) {
-		unsigned* sKeys = smem + L::kKeys + slot * TILE;
-		const long long tileStart = (long long)tile * TILE;
-		const int count = (int)min((long long)TILE, (long long)a.n - tileStart);
-		const bool bulk = tile_is_bulk(tile);
-		const int next = tile + 1;
+	for(long long tileStart = begin; tileStart < end; tileStart += TILE) {
+		unsigned* sKeys = sm.keys(slot);
+		const int count = (int)min((long long)TILE, end - tileStart);
+		const bool bulk = tile_is_bulk(tileStart);
+		const long long next = tileStart + TILE;
 
 		// The next tile's keys go into the other slot (free since the end of
 		// the previous iteration) while this one is sorted.
-		if(KSLOTS == 2 && tid == 0 && next < t1 && tile_is_bulk(next)) {
+		if(KSLOTS == 2 && tid == 0 && next < end && tile_is_bulk(next)) {
 			fence_proxy_async_smem();
-			stage_tile(smem + L::kKeys + (slot ^ 1) * TILE,
-				a.buf.keysIn + (size_t)next * TILE, kTileBytes, &sBar[slot ^ 1]);
+			stage_tile(sm.keys(slot ^ 1), a.buf.keysIn + next, kTileBytes, &sBar[slot ^ 1]);
 		}
 
 		unsigned* myHist = sWarpHist + warp * kDigitBins;
@@ -503,10 +539,10 @@ sort_kernel(const SortArgs a) {
 			if(!mbar_wait_bounded(&sBar[slot], (phase >> slot) & 1u))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 			phase ^= 1u << slot;
-			rank_tile<IPT, true>(sKeys, myHist, warpBase, lane, count, shift, mask,
+			rank_tile<IPT, true, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
-			// Plain loads (a partial tile, or buffers that are not 16-byte
+			// Plain loads (a partial tile, or data that is not 16-byte
 			// aligned): stage the keys and the first value array by hand.
 			for(int i = tid; i < TILE; i += NT) {
 				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
@@ -514,7 +550,7 @@ sort_kernel(const SortArgs a) {
 					sVals[i] = i < count ? a.buf.valsIn[0][tileStart + i] : 0u;
 			}
 			__syncthreads();
-			rank_tile<IPT, false>(sKeys, myHist, warpBase, lane, count, shift, mask,
+			rank_tile<IPT, false, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -569,7 +605,7 @@ sort_kernel(const SortArgs a) {
 		if constexpr(VM == kValueIndex) {
 #pragma unroll
 			for(int i = 0; i < IPT; ++i)
-				sVals[rank[i]] = (unsigned)(tileStart + warpBase + i * 32 + lane);
+				sVals[rank[i]] = (unsigned)(tileStart - indexBase + warpBase + i * 32 + lane);
 		}
 		if constexpr(NV >= 1) {
 			unsigned vals[IPT];
@@ -591,7 +627,7 @@ sort_kernel(const SortArgs a) {
 				stage_tile(sStream, a.buf.valsIn[1] + tileStart, kTileBytes, &sBar[3]);
 			}
 		}
-		if(tile == a.failTile && tid == 0) {
+		if(a.failTile >= 0 && tileStart / TILE == a.failTile && tid == 0) {
 			// Injected fault (tests only): wait on a barrier that nothing
 			// completes, so the bounded wait runs out and is reported.
 			if(!mbar_wait_bounded(&sBar[5], 0))
@@ -606,7 +642,7 @@ sort_kernel(const SortArgs a) {
 			for(int j = 0; j < IPT; ++j) {
 				const int p = j * NT + tid;
 				const unsigned k = sKeys[p];
-				const int dst = sScatter[(k >> shift) & mask] + p;
+				const int dst = sScatter[digit(k)] + p;
 				a.buf.keysOut[dst] = k;
 				if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
 			}
@@ -616,7 +652,7 @@ sort_kernel(const SortArgs a) {
 				const int p = j * NT + tid;
 				if(p < count) {
 					const unsigned k = sKeys[p];
-					const int dst = sScatter[(k >> shift) & mask] + p;
+					const int dst = sScatter[digit(k)] + p;
 					a.buf.keysOut[dst] = k;
 					if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
 				}
@@ -657,7 +693,7 @@ sort_kernel(const SortArgs a) {
 			for(int j = 0; j < IPT; ++j) {
 				const int p = j * NT + tid;
 				if(p < count) {
-					const int dst = sScatter[(sKeys[p] >> shift) & mask] + p;
+					const int dst = sScatter[digit(sKeys[p])] + p;
 					a.buf.valsOut[v][dst] = sVals[p];
 				}
 			}
@@ -668,15 +704,431 @@ sort_kernel(const SortArgs a) {
 
 		// This tile's buffers are free: request the next tile's first value
 		// array, and with one key slot its keys.
-		if(tid == 0 && next < t1 && tile_is_bulk(next)) {
+		if(tid == 0 && next < end && tile_is_bulk(next)) {
 			fence_proxy_async_smem();
-			if(KSLOTS == 1)
-				stage_tile(sKeys, a.buf.keysIn + (size_t)next * TILE, kTileBytes, &sBar[0]);
+			if(KSLOTS == 1) stage_tile(sKeys, a.buf.keysIn + next, kTileBytes, &sBar[0]);
 			if constexpr(NV >= 1)
-				stage_tile(sVals, a.buf.valsIn[0] + (size_t)next * TILE, kTileBytes,
-					&sBar[2]);
+				stage_tile(sVals, a.buf.valsIn[0] + next, kTileBytes, &sBar[2]);
 		}
 		slot = KSLOTS == 2 ? slot ^ 1 : 0;
+	}
+}
+
+// One pass over a whole array: CTA r sorts range r of the split.
+template<int VM, bool BYTE>
+__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
+sort_kernel(const SortArgs a) {
+	using L = SortLayout<VM>;
+	extern __shared__ __align__(128) unsigned smem[];
+	const SortSmem<VM> sm(smem);
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const int warp = tid >> 5;
+	const int r = blockIdx.x;
+	const int R = a.split.numRanges;
+	const long long begin = (long long)a.split.first_tile(r) * L::TILE;
+	const long long end = min((long long)a.n, (long long)a.split.first_tile(r + 1) * L::TILE);
+
+	// Each digit starts at the keys with smaller digits in the whole array
+	// plus the keys with this digit in the ranges before this one.
+	const unsigned total = tid < kDigitBins ? a.totals[tid] : 0u;
+	const unsigned inclTotal = warp_inclusive_scan(total, lane);
+	if(lane == 31 && tid < kDigitBins) sm.scan[warp] = inclTotal;
+	const int nonEmpty = __syncthreads_count(tid < kDigitBins && total != 0);
+	if(tid < kDigitBins) {
+		unsigned prefix = 0;
+		for(int w = 0; w < warp; ++w) prefix += sm.scan[w];
+		sm.running[tid] = prefix + inclTotal - total + a.rangeOffsets[(size_t)tid * R + r];
+	}
+	if(nonEmpty <= 1) {
+		copy_range<VM>(a, begin, end, 0);
+		return;
+	}
+	sort_setup<VM>(sm);
+	__syncthreads();
+	unsigned phase = 0;
+	sort_range<VM, BYTE>(a, sm, begin, end, 0, phase);
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Segmented sort: many independent segments of one array, one pass plan.
+//
+// seg_plan_kernel classifies the segments (device offsets) once per sort:
+// segments of at most kSegSmallMax elements go to a kernel that sorts each
+// one in shared memory through every pass (tiny ones with a small tile);
+// larger ones are cut into ranges of consecutive tiles. Each pass then runs
+// seg_count (range digit counts), seg_scan (per segment: digit starts and
+// range offsets, plus whether the segment has a single digit) and seg_sort
+// (the range sort loop of the one-array path). All of them are persistent
+// over device-side work lists, so the launch shapes do not depend on the
+// segment sizes.
+
+constexpr int kSegTinyMax = 512;
+constexpr int kSegSmallMax = 4096;
+constexpr int kSegMaxRangesPerSegment = 64;
+constexpr int kSegTilesPerRange = 4;
+constexpr int kPlanThreads = 1024;
+
+// counters: [0] tiny segments, [1] small, [2] large, [3] ranges, [4] error.
+struct SegPlanArgs {
+	const int* offsets;
+	int numSegments;
+	int n;
+	int tile;
+	int* tinyList;
+	int* smallList;
+	int* largeList;
+	int* largeRangeFirst;
+	int* largeRangeCount;
+	int* rangeBegin;
+	int* rangeEnd;
+	int* rangeSeg;
+	int* counters;
+	unsigned* devError;
+	volatile unsigned* hostError;
+};
+
+__device__ __forceinline__ void seg_classify(const SegPlanArgs& a, int s, int& tiny,
+	int& small, int& large, int& ranges) {
+	const int len = a.offsets[s + 1] - a.offsets[s];
+	tiny = small = large = ranges = 0;
+	// A one-element segment still moves to the result buffers (and gets its
+	// index in index mode).
+	if(len <= 0) return;
+	if(len <= kSegTinyMax) tiny = 1;
+	else if(len <= kSegSmallMax) small = 1;
+	else {
+		large = 1;
+		const int tiles = (len + a.tile - 1) / a.tile;
+		ranges = min(kSegMaxRangesPerSegment,
+			(tiles + kSegTilesPerRange - 1) / kSegTilesPerRange);
+	}
+}
+
+// Exclusive scan over the 1024 threads of the plan kernel.
+__device__ __forceinline__ int block_exclusive_scan(int x, int* sScan, int& total) {
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	int incl = (int)warp_inclusive_scan((unsigned)x, lane);
+	__syncthreads();
+	if(lane == 31) sScan[warp] = incl;
+	__syncthreads();
+	if(warp == 0) {
+		int w = sScan[lane];
+		int wi = (int)warp_inclusive_scan((unsigned)w, lane);
+		sScan[lane] = wi - w;
+		if(lane == 31) sScan[32] = wi;
+	}
+	__syncthreads();
+	total = sScan[32];
+	return sScan[warp] + incl - x;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) seg_plan_kernel(const SegPlanArgs a) {
+	__shared__ int sScan[33];
+	const int tid = threadIdx.x;
+	const int S = a.numSegments;
+	const int chunk = (S + kPlanThreads - 1) / kPlanThreads;
+	const int s0 = min(S, tid * chunk);
+	const int s1 = min(S, s0 + chunk);
+
+	// Offsets must start at 0, never decrease and end at n.
+	bool bad = false;
+	for(int s = s0; s < s1; ++s) bad |= a.offsets[s + 1] < a.offsets[s];
+	if(tid == 0) bad |= a.offsets[0] != 0 || a.offsets[S] != a.n;
+	if(__syncthreads_or(bad)) {
+		if(tid == 0) {
+			for(int i = 0; i < 5; ++i) a.counters[i] = 0;
+			report_error(a.devError, a.hostError, kErrBadSegments);
+		}
+		return;
+	}
+
+	int nt = 0, ns = 0, nl = 0, nr = 0;
+	for(int s = s0; s < s1; ++s) {
+		int t, sm, l, r;
+		seg_classify(a, s, t, sm, l, r);
+		nt += t;
+		ns += sm;
+		nl += l;
+		nr += r;
+	}
+	int totT, totS, totL, totR;
+	int bt = block_exclusive_scan(nt, sScan, totT);
+	int bs = block_exclusive_scan(ns, sScan, totS);
+	int bl = block_exclusive_scan(nl, sScan, totL);
+	int br = block_exclusive_scan(nr, sScan, totR);
+	for(int s = s0; s < s1; ++s) {
+		int t, sm, l, r;
+		seg_classify(a, s, t, sm, l, r);
+		if(t) a.tinyList[bt++] = s;
+		if(sm) a.smallList[bs++] = s;
+		if(l) {
+			a.largeList[bl] = s;
+			a.largeRangeFirst[bl] = br;
+			a.largeRangeCount[bl] = r;
+			++bl;
+			// Split the segment's tiles evenly over its r ranges.
+			const int begin = a.offsets[s];
+			const int end = a.offsets[s + 1];
+			const int tiles = (end - begin + a.tile - 1) / a.tile;
+			const int lo = tiles / r;
+			const int extra = tiles % r;
+			for(int k = 0; k < r; ++k) {
+				const int t0 = k * lo + min(k, extra);
+				const int t1 = (k + 1) * lo + min(k + 1, extra);
+				a.rangeBegin[br] = (int)(begin + (long long)t0 * a.tile);
+				a.rangeEnd[br] = (int)min((long long)end, begin + (long long)t1 * a.tile);
+				a.rangeSeg[br] = s;
+				++br;
+			}
+		}
+	}
+	if(tid == 0) {
+		a.counters[0] = totT;
+		a.counters[1] = totS;
+		a.counters[2] = totL;
+		a.counters[3] = totR;
+	}
+}
+
+struct SegCountArgs {
+	const unsigned* keys;
+	const int* rangeBegin;
+	const int* rangeEnd;
+	const int* counters;
+	int shift;
+	int width;
+	int vecOk;
+	unsigned* counts;               // [R][256], range-major
+};
+
+__global__ void __launch_bounds__(kCountThreads) seg_count_kernel(const SegCountArgs a) {
+	__shared__ unsigned sHist[kDigitBins * 32];
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const unsigned mask = (1u << a.width) - 1;
+	const int shift = a.shift;
+	const int R = a.counters[3];
+	unsigned* myCol = sHist + lane;
+	auto add = [&](unsigned k) { atomicAdd(&myCol[((k >> shift) & mask) * 32], 1u); };
+
+	for(int r = blockIdx.x; r < R; r += gridDim.x) {
+		for(int i = tid; i < kDigitBins * 32; i += kCountThreads) sHist[i] = 0;
+		__syncthreads();
+		const int begin = a.rangeBegin[r];
+		const int end = a.rangeEnd[r];
+		int e = begin;
+		if(a.vecOk) {
+			// Plain loads up to a 16-byte boundary, then 16-byte loads.
+			const int head = min(end, (begin + 3) & ~3);
+			for(int i = begin + tid; i < head; i += kCountThreads) add(a.keys[i]);
+			const uint4* src = reinterpret_cast<const uint4*>(a.keys + head);
+			const int nvec = max(0, (end - head) / 4);
+			for(int i = tid; i < nvec; i += kCountThreads) {
+				const uint4 q = ld_stream_u4(src + i);
+				add(q.x);
+				add(q.y);
+				add(q.z);
+				add(q.w);
+			}
+			e = head + 4 * nvec;
+		}
+		for(int i = e + tid; i < end; i += kCountThreads) add(a.keys[i]);
+		__syncthreads();
+		for(int b = tid >> 5; b < kDigitBins; b += kCountThreads / 32) {
+			unsigned c = sHist[b * 32 + lane];
+#pragma unroll
+			for(int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+			if(lane == 0) a.counts[(size_t)r * kDigitBins + b] = c;
+		}
+		__syncthreads();
+	}
+}
+
+struct SegScanArgs {
+	const int* offsets;
+	const int* largeList;
+	const int* largeRangeFirst;
+	const int* largeRangeCount;
+	const int* counters;
+	const unsigned* counts;         // [R][256]
+	unsigned* rangeStart;           // [R][256]: first output position per digit
+	unsigned* rangeTrivial;         // [R]: the segment has a single digit
+};
+
+// One CTA per large segment: digit d of range r starts at segment start +
+// keys of the segment with smaller digits + keys with digit d in the
+// segment's earlier ranges.
+__global__ void __launch_bounds__(256) seg_scan_kernel(const SegScanArgs a) {
+	__shared__ unsigned sScan[8];
+	const int d = threadIdx.x;
+	const int lane = d & 31;
+	const int warp = d >> 5;
+	const int L = a.counters[2];
+	for(int i = blockIdx.x; i < L; i += gridDim.x) {
+		const int s = a.largeList[i];
+		const int r0 = a.largeRangeFirst[i];
+		const int nr = a.largeRangeCount[i];
+		unsigned run = 0;
+		for(int k = 0; k < nr; ++k) {
+			const size_t at = (size_t)(r0 + k) * kDigitBins + d;
+			const unsigned c = a.counts[at];
+			a.rangeStart[at] = run;
+			run += c;
+		}
+		const unsigned incl = warp_inclusive_scan(run, lane);
+		if(lane == 31) sScan[warp] = incl;
+		const int nonEmpty = __syncthreads_count(run != 0);
+		unsigned prefix = 0;
+		for(int w = 0; w < warp; ++w) prefix += sScan[w];
+		const unsigned base = (unsigned)a.offsets[s] + prefix + incl - run;
+		for(int k = 0; k < nr; ++k) {
+			const size_t at = (size_t)(r0 + k) * kDigitBins + d;
+			a.rangeStart[at] += base;
+		}
+		if(d < nr) a.rangeTrivial[r0 + d] = nonEmpty <= 1;
+		for(int k = d + 256; k < nr; k += 256) a.rangeTrivial[r0 + k] = nonEmpty <= 1;
+		__syncthreads();
+	}
+}
+
+struct SegSortArgs {
+	SortArgs sort;                  // buffers, digit, bulk flag, errors
+	const int* offsets;
+	const int* rangeBegin;
+	const int* rangeEnd;
+	const int* rangeSeg;
+	const int* counters;
+	const unsigned* rangeStart;
+	const unsigned* rangeTrivial;
+};
+
+template<int VM, bool BYTE>
+__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
+seg_sort_kernel(const SegSortArgs a) {
+	extern __shared__ __align__(128) unsigned smem[];
+	const SortSmem<VM> sm(smem);
+	const int tid = threadIdx.x;
+	const int R = a.counters[3];
+	sort_setup<VM>(sm);
+	unsigned phase = 0;
+	for(int r = blockIdx.x; r < R; r += gridDim.x) {
+		const long long begin = a.rangeBegin[r];
+		const long long end = a.rangeEnd[r];
+		const long long segStart = a.offsets[a.rangeSeg[r]];
+		if(tid < kDigitBins) sm.running[tid] = a.rangeStart[(size_t)r * kDigitBins + tid];
+		const bool trivial = a.rangeTrivial[r] != 0;
+		__syncthreads();
+		if(trivial) copy_range<VM>(a.sort, begin, end, segStart);
+		else sort_range<VM, BYTE>(a.sort, sm, begin, end, segStart, phase);
+		__syncthreads();
+	}
+}
+
+// Segments of at most TILE elements, sorted whole in shared memory: keys
+// and their segment-local positions go through every pass, then keys are
+// written out and each value array is permuted through shared memory by
+// the final positions (index mode writes the positions).
+constexpr int kSmallThreads = 256;
+
+struct SmallSortArgs {
+	PassBuffers buf;                // in: [0] arrays; out: the result arrays
+	PassPlan plan;
+	const int* offsets;
+	const int* list;
+	const int* counters;
+	int listIndex;                  // counters[listIndex] = list length
+	int numArrays;                  // value arrays to permute (0 in index mode)
+	int indexMode;
+};
+
+template<int IPT>
+__global__ void __launch_bounds__(kSmallThreads) small_sort_kernel(const SmallSortArgs a) {
+	constexpr int NT = kSmallThreads;
+	constexpr int TILE = NT * IPT;
+	constexpr int NW = NT / 32;
+	__shared__ unsigned sKeys[TILE];
+	__shared__ unsigned sIdx[TILE];
+	__shared__ unsigned sWarpHist[NW * kDigitBins];
+	__shared__ unsigned sScan[32];
+
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const int warp = tid >> 5;
+	const int warpBase = warp * 32 * IPT;
+	const unsigned ltMask = lanemask_lt();
+	unsigned nClear[4];
+#pragma unroll
+	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
+	const int count = a.counters[a.listIndex];
+
+	for(int i = blockIdx.x; i < count; i += gridDim.x) {
+		const int s = a.list[i];
+		const int begin = a.offsets[s];
+		const int len = a.offsets[s + 1] - begin;
+		for(int j = tid; j < TILE; j += NT) {
+			sKeys[j] = j < len ? a.buf.keysIn[begin + j] : 0xffffffffu;
+			sIdx[j] = j;
+		}
+		for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
+		__syncthreads();
+
+		for(int p = 0; p < a.plan.numPasses; ++p) {
+			const DigitOf<false> digit(a.plan.shift[p], a.plan.width[p]);
+			unsigned rank[IPT];
+			rank_tile<IPT, false, false>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
+				lane, len, digit, ltMask, nClear, rank);
+			__syncthreads();
+			unsigned c[NW];
+			unsigned tileTotal = 0;
+#pragma unroll
+			for(int w = 0; w < NW; ++w) {
+				c[w] = sWarpHist[w * kDigitBins + tid];
+				tileTotal += c[w];
+			}
+			const unsigned incl = warp_inclusive_scan(tileTotal, lane);
+			if(lane == 31) sScan[warp] = incl;
+			__syncthreads();
+			unsigned prefix = 0;
+			for(int w = 0; w < warp; ++w) prefix += sScan[w];
+			unsigned run = prefix + incl - tileTotal;
+#pragma unroll
+			for(int w = 0; w < NW; ++w) {
+				sWarpHist[w * kDigitBins + tid] = run;
+				run += c[w];
+			}
+			unsigned keys[IPT], idx[IPT];
+#pragma unroll
+			for(int j = 0; j < IPT; ++j) {
+				keys[j] = sKeys[warpBase + j * 32 + lane];
+				idx[j] = sIdx[warpBase + j * 32 + lane];
+			}
+			__syncthreads();
+#pragma unroll
+			for(int j = 0; j < IPT; ++j) {
+				const unsigned pos = (rank[j] & 0xffffu)
+					+ sWarpHist[warp * kDigitBins + (rank[j] >> 16)];
+				sKeys[pos] = keys[j];
+				sIdx[pos] = idx[j];
+			}
+			__syncthreads();
+			for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
+			__syncthreads();
+		}
+
+		for(int j = tid; j < len; j += NT) {
+			a.buf.keysOut[begin + j] = sKeys[j];
+			if(a.indexMode) a.buf.valsOut[0][begin + j] = sIdx[j];
+		}
+		for(int v = 0; v < a.numArrays; ++v) {
+			// Stage the segment's values (the input may be the output buffer).
+			__syncthreads();
+			for(int j = tid; j < len; j += NT) sKeys[j] = a.buf.valsIn[v][begin + j];
+			__syncthreads();
+			for(int j = tid; j < len; j += NT) a.buf.valsOut[v][begin + j] = sKeys[sIdx[j]];
+		}
+		__syncthreads();
 	}
 }
 
@@ -691,8 +1143,13 @@ __global__ void iota_kernel(unsigned* out, int n) {
 
 template<int VM>
 static cudaError_t set_sort_attributes() {
-	return cudaFuncSetAttribute(sort_kernel<VM>,
-		cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SortLayout<VM>::kBytes);
+	const int bytes = (int)SortLayout<VM>::kBytes;
+	const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+	cudaError_t e = cudaFuncSetAttribute(sort_kernel<VM, false>, attr, bytes);
+	if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true>, attr, bytes);
+	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
+	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
+	return e;
 }
 
 cudaError_t configure_kernels() {
@@ -710,8 +1167,12 @@ cudaError_t configure_kernels() {
 }
 
 int pass_tile_elements(int valueMode) {
-	(void)valueMode;
-	return kTileElements;
+	switch(valueMode) {
+		case -1: return SortLayout<-1>::TILE;
+		case 0: return SortLayout<0>::TILE;
+		case 1: return SortLayout<1>::TILE;
+		default: return SortLayout<2>::TILE;
+	}
 }
 
 size_t pass_scratch_bytes() {
@@ -741,7 +1202,7 @@ static int sort_ctas_per_sm() {
 	static int perSM = 0;
 	if(!perSM) {
 		int v = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, sort_kernel<VM>,
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, sort_kernel<VM, false>,
 			SortLayout<VM>::NT, SortLayout<VM>::kBytes);
 		perSM = v > 0 ? v : 1;
 	}
@@ -783,6 +1244,7 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	CountArgs c;
 	c.keys = buf.keysIn;
 	c.n = n;
+	c.tile = pass_tile_elements(valueMode);
 	c.shift = plan.shift[pass];
 	c.width = plan.width[pass];
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
@@ -802,7 +1264,10 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 template<int VM>
 static void launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
 	using L = SortLayout<VM>;
-	sort_kernel<VM><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
+	if(a.width == 8 && (a.shift & 7) == 0)
+		sort_kernel<VM, true><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
+	else
+		sort_kernel<VM, false><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
 }
 
 cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
@@ -844,6 +1309,180 @@ cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
 	if(e != cudaSuccess) return e;
 	return launch_pass_sort(buf, valueMode, n, pass, plan, ctrl, scratch, useBulk,
 		failTile, hostError, numSMs, stream);
+}
+
+// Segmented scratch: [counters 8][lists 5 x S][range table 4 x Rmax]
+// [counts Rmax x 256][rangeStart Rmax x 256], in 32-bit words.
+struct SegScratch {
+	int* counters;
+	int* tinyList;
+	int* smallList;
+	int* largeList;
+	int* largeRangeFirst;
+	int* largeRangeCount;
+	int* rangeBegin;
+	int* rangeEnd;
+	int* rangeSeg;
+	unsigned* rangeTrivial;
+	unsigned* counts;
+	unsigned* rangeStart;
+};
+
+static size_t seg_max_ranges(int n, int numSegments) {
+	return (size_t)n / SortLayout<2>::TILE + (size_t)numSegments + 1;
+}
+
+size_t seg_scratch_bytes(int n, int numSegments) {
+	const size_t S = (size_t)numSegments;
+	const size_t R = seg_max_ranges(n, numSegments);
+	return sizeof(unsigned) * (8 + 5 * S + 4 * R + 2 * R * kDigitBins) + 256;
+}
+
+static SegScratch seg_scratch(void* base, int n, int numSegments) {
+	const size_t S = (size_t)numSegments;
+	const size_t R = seg_max_ranges(n, numSegments);
+	unsigned* w = static_cast<unsigned*>(base);
+	SegScratch x;
+	x.counters = reinterpret_cast<int*>(w); w += 8;
+	x.tinyList = reinterpret_cast<int*>(w); w += S;
+	x.smallList = reinterpret_cast<int*>(w); w += S;
+	x.largeList = reinterpret_cast<int*>(w); w += S;
+	x.largeRangeFirst = reinterpret_cast<int*>(w); w += S;
+	x.largeRangeCount = reinterpret_cast<int*>(w); w += S;
+	x.rangeBegin = reinterpret_cast<int*>(w); w += R;
+	x.rangeEnd = reinterpret_cast<int*>(w); w += R;
+	x.rangeSeg = reinterpret_cast<int*>(w); w += R;
+	x.rangeTrivial = w; w += R;
+	x.counts = w; w += R * kDigitBins;
+	x.rangeStart = w;
+	return x;
+}
+
+cudaError_t launch_seg_plan(const int* offsets, int numSegments, int n,
+	int valueMode, void* scratch, Control* ctrl, volatile unsigned* hostError,
+	cudaStream_t stream) {
+	const SegScratch x = seg_scratch(scratch, n, numSegments);
+	SegPlanArgs a;
+	a.offsets = offsets;
+	a.numSegments = numSegments;
+	a.n = n;
+	a.tile = pass_tile_elements(valueMode);
+	a.tinyList = x.tinyList;
+	a.smallList = x.smallList;
+	a.largeList = x.largeList;
+	a.largeRangeFirst = x.largeRangeFirst;
+	a.largeRangeCount = x.largeRangeCount;
+	a.rangeBegin = x.rangeBegin;
+	a.rangeEnd = x.rangeEnd;
+	a.rangeSeg = x.rangeSeg;
+	a.counters = x.counters;
+	a.devError = &ctrl->error;
+	a.hostError = hostError;
+	seg_plan_kernel<<<1, kPlanThreads, 0, stream>>>(a);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_seg_small(const PassBuffers& buf, int valueMode,
+	const PassPlan& plan, const int* offsets, int numSegments, int n,
+	void* scratch, int numSMs, cudaStream_t stream) {
+	const SegScratch x = seg_scratch(scratch, n, numSegments);
+	SmallSortArgs a;
+	a.buf = buf;
+	a.plan = plan;
+	a.offsets = offsets;
+	a.counters = x.counters;
+	a.numArrays = valueMode > 0 ? valueMode : 0;
+	a.indexMode = valueMode == kValueIndex;
+	a.list = x.tinyList;
+	a.listIndex = 0;
+	small_sort_kernel<kSegTinyMax / kSmallThreads><<<numSMs * 8, kSmallThreads, 0,
+		stream>>>(a);
+	a.list = x.smallList;
+	a.listIndex = 1;
+	small_sort_kernel<kSegSmallMax / kSmallThreads><<<numSMs * 4, kSmallThreads, 0,
+		stream>>>(a);
+	return cudaGetLastError();
+}
+
+template<int VM>
+static int seg_sort_ctas_per_sm() {
+	static int perSM = 0;
+	if(!perSM) {
+		int v = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, seg_sort_kernel<VM, false>,
+			SortLayout<VM>::NT, SortLayout<VM>::kBytes);
+		perSM = v > 0 ? v : 1;
+	}
+	return perSM;
+}
+
+template<int VM>
+static void launch_seg_sort_vm(const SegSortArgs& a, int numSMs, cudaStream_t stream) {
+	using L = SortLayout<VM>;
+	const int grid = numSMs * seg_sort_ctas_per_sm<VM>();
+	if(a.sort.width == 8 && (a.sort.shift & 7) == 0)
+		seg_sort_kernel<VM, true><<<grid, L::NT, L::kBytes, stream>>>(a);
+	else
+		seg_sort_kernel<VM, false><<<grid, L::NT, L::kBytes, stream>>>(a);
+}
+
+cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
+	const PassPlan& plan, const int* offsets, int numSegments, int n,
+	void* scratch, Control* ctrl, bool useBulk, volatile unsigned* hostError,
+	int numSMs, cudaStream_t stream) {
+	const SegScratch x = seg_scratch(scratch, n, numSegments);
+	SegCountArgs c;
+	c.keys = buf.keysIn;
+	c.rangeBegin = x.rangeBegin;
+	c.rangeEnd = x.rangeEnd;
+	c.counters = x.counters;
+	c.shift = plan.shift[pass];
+	c.width = plan.width[pass];
+	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
+	c.counts = x.counts;
+	seg_count_kernel<<<numSMs * 4, kCountThreads, 0, stream>>>(c);
+
+	SegScanArgs q;
+	q.offsets = offsets;
+	q.largeList = x.largeList;
+	q.largeRangeFirst = x.largeRangeFirst;
+	q.largeRangeCount = x.largeRangeCount;
+	q.counters = x.counters;
+	q.counts = x.counts;
+	q.rangeStart = x.rangeStart;
+	q.rangeTrivial = x.rangeTrivial;
+	seg_scan_kernel<<<numSMs * 8, 256, 0, stream>>>(q);
+
+	SegSortArgs a;
+	a.sort.buf = buf;
+	a.sort.rangeOffsets = nullptr;
+	a.sort.totals = nullptr;
+	a.sort.devError = &ctrl->error;
+	a.sort.hostError = hostError;
+	a.sort.n = n;
+	a.sort.shift = plan.shift[pass];
+	a.sort.width = plan.width[pass];
+	a.sort.useBulk = useBulk ? 1 : 0;
+	a.sort.failTile = -1;
+	a.offsets = offsets;
+	a.rangeBegin = x.rangeBegin;
+	a.rangeEnd = x.rangeEnd;
+	a.rangeSeg = x.rangeSeg;
+	a.counters = x.counters;
+	a.rangeStart = x.rangeStart;
+	a.rangeTrivial = x.rangeTrivial;
+	switch(valueMode) {
+		case -1: launch_seg_sort_vm<-1>(a, numSMs, stream); break;
+		case 0: launch_seg_sort_vm<0>(a, numSMs, stream); break;
+		case 1: launch_seg_sort_vm<1>(a, numSMs, stream); break;
+		case 2: launch_seg_sort_vm<2>(a, numSMs, stream); break;
+		case 3: launch_seg_sort_vm<3>(a, numSMs, stream); break;
+		case 4: launch_seg_sort_vm<4>(a, numSMs, stream); break;
+		case 5: launch_seg_sort_vm<5>(a, numSMs, stream); break;
+		case 6: launch_seg_sort_vm<6>(a, numSMs, stream); break;
+		default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
 }
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream) {

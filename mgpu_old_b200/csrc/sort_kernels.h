@@ -97,6 +97,28 @@ cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
 	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
 	cudaStream_t stream);
 
+// Segmented sort (sortSegmentedArray). Device scratch for n elements in
+// numSegments segments; all three launchers take the same scratch.
+size_t seg_scratch_bytes(int n, int numSegments);
+
+// Classify the segments of device `offsets` (numSegments + 1 entries) into
+// the work lists in scratch. Bad offsets set an error and empty lists.
+cudaError_t launch_seg_plan(const int* offsets, int numSegments, int n,
+	int valueMode, void* scratch, Control* ctrl, volatile unsigned* hostError,
+	cudaStream_t stream);
+
+// Sort every segment of at most 4096 elements through all passes of `plan`,
+// from buf.*In into buf.*Out (which may alias).
+cudaError_t launch_seg_small(const PassBuffers& buf, int valueMode,
+	const PassPlan& plan, const int* offsets, int numSegments, int n,
+	void* scratch, int numSMs, cudaStream_t stream);
+
+// One pass over the larger segments (count, scan and sort kernels).
+cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
+	const PassPlan& plan, const int* offsets, int numSegments, int n,
+	void* scratch, Control* ctrl, bool useBulk, volatile unsigned* hostError,
+	int numSMs, cudaStream_t stream);
+
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream);
 
 } // namespace mgpusort

@@ -66,11 +66,56 @@ def pairs_uniform32(n: int = 1 << 26, seed: int = 5) -> SortCase:
                     _u32(rng, n), [np.arange(n, dtype=np.uint32)], 1, 0, 32)
 
 
+def lognormal_segment_sizes(num_segments: int = 10_000, median: float = 2048.0,
+                            sigma: float = 2.0, lo: int = 1, hi: int = 4_194_304,
+                            seed: int = 4) -> np.ndarray:
+    """Segment sizes round(lognormal(ln median, sigma)) clipped to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    sizes = np.rint(rng.lognormal(np.log(median), sigma, num_segments))
+    return np.clip(sizes, lo, hi).astype(np.int64)
+
+
+@dataclass
+class SegmentedCase(SortCase):
+    offsets: np.ndarray = None   # int32, num_segments + 1 boundaries
+
+    @property
+    def num_segments(self) -> int:
+        return int(self.offsets.size - 1)
+
+
+def segments_lognormal(num_segments: int = 10_000, seed: int = 4,
+                       scale_to: int | None = None) -> SegmentedCase:
+    """Batched segmented sort: lognormal segment sizes (median 2048, sigma 2,
+    clipped to [1, 4194304]), uniform 32-bit keys, value = index within the
+    segment, bits [0, 32). scale_to rescales the sizes to that total."""
+    sizes = lognormal_segment_sizes(num_segments, seed=seed)
+    if scale_to:
+        sizes = np.maximum(1, np.rint(sizes * (scale_to / sizes.sum()))).astype(np.int64)
+    offsets = np.zeros(sizes.size + 1, np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    n = int(offsets[-1])
+    keys = _u32(_rng(seed + 100), n)
+    local = (np.arange(n, dtype=np.int64) - np.repeat(offsets[:-1], sizes)).astype(np.uint32)
+    name = f"segments_{num_segments}_lognormal" + (f"_scaled{scale_to}" if scale_to else "")
+    return SegmentedCase(name, keys, [local], 1, 0, 32, offsets.astype(np.int32))
+
+
+def keys_uniform32_64m() -> SortCase:
+    """Keys-only, uniform over 32 bits, 64Mi keys (a large keys-only case)."""
+    c = keys_uniform32(1 << 26, seed=6)
+    c.name = "keys_u32_64M"
+    return c
+
+
 WORKLOADS = {
     "keys_u32_1M": keys_uniform32,
     "pairs_and24_32M": pairs_and24,
     "multi6_17bit_16M": multi6_17bit,
     "pairs_u32_64M": pairs_uniform32,
+    "keys_u32_64M": keys_uniform32_64m,
+    "segments_10k": segments_lognormal,
+    "segments_10k_64M": lambda: segments_lognormal(scale_to=1 << 26),
 }
 
 

@@ -22,7 +22,8 @@
 //    also the timed CPU baseline.
 //
 // Both must agree with each other, with the reference's own cpusort.cpp
-// built here (oracle/build_ref.sh) on the keys it can sort, and with the GPU.
+// built here (oracle/Makefile, `make ref`) on the keys it can sort, and with
+// the GPU.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -172,6 +173,32 @@ int oracle_sort_lsd(uint32_t* keys, uint32_t* const* vals, int valueCount,
 		std::memcpy(keys, kA, sizeof(uint32_t) * n);
 		for(int v = 0; v < arrays; ++v)
 			std::memcpy(vals[v], vA[v], sizeof(uint32_t) * n);
+	}
+	return 0;
+}
+
+// Batched segmented sort: every segment [offsets[i], offsets[i + 1]) sorted
+// on its own exactly as oracle_sort_stable sorts one array (index mode:
+// positions within the segment). This is what one sortArray call per
+// segment computes. Returns 0, or -1 for invalid arguments.
+int oracle_sort_segments(const uint32_t* keys, const uint32_t* const* vals,
+	int valueCount, const int* offsets, int numSegments, int firstBit,
+	int endBit, uint32_t* keysOut, uint32_t* const* valsOut) {
+	if(numSegments < 0 || valueCount < -1 || valueCount > 6) return -1;
+	const int arrays = num_arrays(valueCount);
+	for(int s = 0; s < numSegments; ++s) {
+		const int b = offsets[s];
+		const int len = offsets[s + 1] - b;
+		if(len < 0) return -1;
+		const uint32_t* vin[6] = {};
+		uint32_t* vout[6] = {};
+		for(int v = 0; v < arrays; ++v) {
+			if(valueCount > 0) vin[v] = vals[v] + b;
+			vout[v] = valsOut[v] + b;
+		}
+		int rc = oracle_sort_stable(keys + b, vin, valueCount, len, firstBit, endBit,
+			keysOut + b, vout);
+		if(rc) return rc;
 	}
 	return 0;
 }

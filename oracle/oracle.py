@@ -42,6 +42,9 @@ def lib() -> ctypes.CDLL:
         l.oracle_sort_lsd.restype = c_int
         l.oracle_sort_lsd.argtypes = [_u32p, POINTER(_u32p), c_int, c_int, c_int,
                                       POINTER(c_int), c_int, c_int, c_int]
+        l.oracle_sort_segments.restype = c_int
+        l.oracle_sort_segments.argtypes = [_u32p, POINTER(_u32p), c_int, POINTER(c_int),
+                                           c_int, c_int, c_int, _u32p, POINTER(_u32p)]
         l.oracle_std_sort_keys.restype = None
         l.oracle_std_sort_keys.argtypes = [_u32p, c_int]
         l.oracle_reference_ex_plan.restype = c_int
@@ -106,6 +109,23 @@ def sort_lsd(keys: np.ndarray, values: list[np.ndarray] | None, value_count: int
     if rc:
         raise ValueError("oracle_sort_lsd: invalid arguments")
     return keys, vals[:arrays]
+
+
+def sort_segments(keys: np.ndarray, values: list[np.ndarray] | None, value_count: int,
+                  offsets: np.ndarray, first_bit: int, end_bit: int):
+    """Each segment sorted on its own (one sortArray per segment)."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint32)
+    vals = [np.ascontiguousarray(v, dtype=np.uint32) for v in (values or [])]
+    offs = np.ascontiguousarray(offsets, dtype=np.int32)
+    arrays = 1 if value_count == -1 else value_count
+    kout = np.empty(keys.size, np.uint32)
+    vout = [np.empty(keys.size, np.uint32) for _ in range(arrays)]
+    rc = lib().oracle_sort_segments(_p(keys), _ptrs(vals), value_count,
+                                    offs.ctypes.data_as(POINTER(c_int)), offs.size - 1,
+                                    first_bit, end_bit, _p(kout), _ptrs(vout))
+    if rc:
+        raise ValueError("oracle_sort_segments: invalid arguments")
+    return kout, vout
 
 
 def reference_ex_plan(num_bits: int, bit_pass: int) -> list[int]:

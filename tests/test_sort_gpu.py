@@ -39,7 +39,10 @@ def test_golden_fixtures(engine, path):
     assert_same(ds, z["expect_keys"], [z[f"expect_values{i}"] for i in range(arrays)])
 
 
-SIZES = [1, 2, 31, 255, 4095, 4096, 4097, 8191, 12289, 100003]
+# Around the tile sizes of the sort kernel (7680 for keys, indices and one
+# value array; 7168 for several value arrays) and of older shapes.
+SIZES = [1, 2, 31, 255, 4095, 4097, 7167, 7168, 7169, 7679, 7680, 7681, 15361,
+         100003]
 
 
 @pytest.mark.parametrize("n", SIZES)
