@@ -65,6 +65,51 @@ sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 sortStatus_t SORTAPI sortSegmentedArray(sortEngine_t engine, sortData_t data,
 	const int* segmentOffsets, int numSegments, CUstream stream);
 
+/* Sort server: requests from host memory are copied in, sorted and copied
+ * back by a scheduler thread that keeps a pool of device memory and one
+ * engine and stream per slot. Requests are admitted in arrival order while a
+ * slot is free and their device footprint (2 x keys + 2 x values) fits the
+ * memory budget; small requests (at most coalesceMax elements) of the same
+ * kind (values or not, same bit range) are coalesced into one segmented sort.
+ * Batches on different slots overlap on the GPU, and requests that arrive
+ * while others are in flight join the next batch (continuous batching). Each
+ * result equals a sortArray of that request alone. No counterpart in the
+ * reference. */
+typedef struct sortServer_d* sortServer_t;
+
+typedef struct {
+	size_t memoryBudget;   /* device bytes for requests in flight; 0: 64 GiB */
+	int slots;             /* batches in flight at once; 0: 4 */
+	int coalesceMax;       /* largest request that is coalesced; 0: 1 Mi */
+	int maxBatchElements;  /* elements per coalesced batch; 0: 16 Mi */
+	int maxBatchRequests;  /* requests per coalesced batch; 0: 4096 */
+} sortServerConfig;
+
+/* Start a server on the current device (config may be NULL). */
+sortStatus_t SORTAPI sortServerCreate(const sortServerConfig* config,
+	sortServer_t* server);
+
+/* Queue a request: sort keys (and values, if non-NULL) by [firstBit,
+ * endBit) into keysOut (valuesOut). All four are host buffers that must stay
+ * valid until the request is waited for; page-locked memory lets the copies
+ * overlap. A request larger than the budget gives
+ * SORT_STATUS_CONFIG_NOT_SUPPORTED. */
+sortStatus_t SORTAPI sortServerSubmit(sortServer_t server, const unsigned* keys,
+	const unsigned* values, int numElements, int firstBit, int endBit,
+	unsigned* keysOut, unsigned* valuesOut, unsigned long long* ticket);
+
+/* *done = 1 once the request's results are in its output buffers. */
+sortStatus_t SORTAPI sortServerPoll(sortServer_t server, unsigned long long ticket,
+	int* done);
+
+/* Block until the request is done; return its status and (if non-NULL) the
+ * seconds from submission to completion. The ticket is retired. */
+sortStatus_t SORTAPI sortServerWait(sortServer_t server, unsigned long long ticket,
+	double* latencySeconds);
+
+/* Finish every queued request, then stop the server and free it. */
+sortStatus_t SORTAPI sortServerDestroy(sortServer_t server);
+
 /* Largest numElements that sortArrayNoAlloc accepts (4 Mi elements). */
 #define SORT_NOALLOC_MAX_ELEMENTS 4194304
 

@@ -55,6 +55,17 @@ class SortData(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    """sortServerConfig (mgpusort_b200.h)."""
+    _fields_ = [
+        ("memoryBudget", ctypes.c_size_t),
+        ("slots", c_int),
+        ("coalesceMax", c_int),
+        ("maxBatchElements", c_int),
+        ("maxBatchRequests", c_int),
+    ]
+
+
 assert ctypes.sizeof(SortData) == 144
 assert SortData.keys.offset == 32 and SortData.values.offset == 48
 
@@ -66,7 +77,8 @@ EXPORTED_SYMBOLS = (
     # mgpusort_b200.h (no reference counterpart)
     "sortArrayAsync", "sortSynchronize", "sortPlanPasses", "sortInjectFault",
     "sortEnableKernelTiming", "sortReadKernelTiming", "sortArrayNoAlloc",
-    "sortSegmentedArray",
+    "sortSegmentedArray", "sortServerCreate", "sortServerSubmit", "sortServerPoll",
+    "sortServerWait", "sortServerDestroy",
 )
 
 # Largest numElements accepted by sortArrayNoAlloc (SORT_NOALLOC_MAX_ELEMENTS).
@@ -109,6 +121,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                          POINTER(ctypes.c_double), POINTER(c_int)]),
         "sortArrayNoAlloc": (c_int, [data_t, c_void_p]),
         "sortSegmentedArray": (c_int, [engine_t, data_t, c_void_p, c_int, c_void_p]),
+        "sortServerCreate": (c_int, [POINTER(ServerConfig), POINTER(c_void_p)]),
+        "sortServerSubmit": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                     c_void_p, c_void_p, POINTER(ctypes.c_ulonglong)]),
+        "sortServerPoll": (c_int, [c_void_p, ctypes.c_ulonglong, POINTER(c_int)]),
+        "sortServerWait": (c_int, [c_void_p, ctypes.c_ulonglong, POINTER(ctypes.c_double)]),
+        "sortServerDestroy": (c_int, [c_void_p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -230,6 +248,50 @@ def sort_array_no_alloc(data: SortData, stream: int = 0) -> int:
     """sortArrayNoAlloc: sortArray without an engine and without allocating;
     waits for the sort. For callers whose device memory is all pre-budgeted."""
     return load_library().sortArrayNoAlloc(ctypes.byref(data), c_void_p(stream))
+
+
+class SortServer:
+    """sortServer_t: submit host-memory sort requests, wait for tickets."""
+
+    def __init__(self, memory_budget: int = 0, slots: int = 0, coalesce_max: int = 0,
+                 max_batch_elements: int = 0, max_batch_requests: int = 0):
+        cfg = ServerConfig(memory_budget, slots, coalesce_max, max_batch_elements,
+                           max_batch_requests)
+        h = c_void_p()
+        check(load_library().sortServerCreate(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, keys_ptr: int, values_ptr: int | None, n: int, first_bit: int,
+               end_bit: int, keys_out_ptr: int, values_out_ptr: int | None) -> int:
+        t = ctypes.c_ulonglong()
+        check(load_library().sortServerSubmit(self._h, c_void_p(keys_ptr),
+                                              c_void_p(values_ptr or 0), n, first_bit,
+                                              end_bit, c_void_p(keys_out_ptr),
+                                              c_void_p(values_out_ptr or 0),
+                                              ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        d = c_int()
+        check(load_library().sortServerPoll(self._h, ticket, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int) -> tuple[int, float]:
+        """(status, seconds from submission to completion)"""
+        lat = ctypes.c_double()
+        st = load_library().sortServerWait(self._h, ticket, ctypes.byref(lat))
+        return st, lat.value
+
+    def close(self) -> None:
+        if self._h:
+            load_library().sortServerDestroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MgpuSortData(SortData):

@@ -21,6 +21,7 @@ SOURCES = [
     "engine.cpp",
     "sort_kernels.cu",
     "noalloc.cu",
+    "server.cpp",
 ]
 
 NVCC_FLAGS = [

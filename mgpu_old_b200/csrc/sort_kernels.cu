@@ -520,11 +520,14 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
 	int slot = 0;
 
-	for(long long tileStart = begin; tileStart < end; tileStart += TILE) {
+	// Tiles lie on a grid of 4-element (16-byte) aligned starts: when begin
+	// is not aligned, the first tile is shorter and every later one can be
+	// staged with bulk copies.
+	for(long long tileStart = begin; tileStart < end;) {
 		unsigned* sKeys = sm.keys(slot);
-		const int count = (int)min((long long)TILE, end - tileStart);
+		const long long next = (tileStart & ~3ll) + TILE;
+		const int count = (int)(min(next, end) - tileStart);
 		const bool bulk = tile_is_bulk(tileStart);
-		const long long next = tileStart + TILE;
 
 		// The next tile's keys go into the other slot (free since the end of
 		// the previous iteration) while this one is sorted.
@@ -711,6 +714,7 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 				stage_tile(sVals, a.buf.valsIn[0] + next, kTileBytes, &sBar[2]);
 		}
 		slot = KSLOTS == 2 ? slot ^ 1 : 0;
+		tileStart = next;
 	}
 }
 
@@ -799,7 +803,8 @@ __device__ __forceinline__ void seg_classify(const SegPlanArgs& a, int s, int& t
 	else if(len <= kSegSmallMax) small = 1;
 	else {
 		large = 1;
-		const int tiles = (len + a.tile - 1) / a.tile;
+		const int base = a.offsets[s] & ~3;
+		const int tiles = (a.offsets[s + 1] - base + a.tile - 1) / a.tile;
 		ranges = min(kSegMaxRangesPerSegment,
 			(tiles + kSegTilesPerRange - 1) / kSegTilesPerRange);
 	}
@@ -868,17 +873,21 @@ __global__ void __launch_bounds__(kPlanThreads) seg_plan_kernel(const SegPlanArg
 			a.largeRangeFirst[bl] = br;
 			a.largeRangeCount[bl] = r;
 			++bl;
-			// Split the segment's tiles evenly over its r ranges.
+			// Split the segment's tiles evenly over its r ranges. Tiles lie on
+			// the 4-element aligned grid from the segment's aligned-down start
+			// (the same grid the sort kernel walks), so the first tile may be
+			// shorter.
 			const int begin = a.offsets[s];
 			const int end = a.offsets[s + 1];
-			const int tiles = (end - begin + a.tile - 1) / a.tile;
+			const long long base = begin & ~3;
+			const int tiles = (int)((end - base + a.tile - 1) / a.tile);
 			const int lo = tiles / r;
 			const int extra = tiles % r;
 			for(int k = 0; k < r; ++k) {
 				const int t0 = k * lo + min(k, extra);
 				const int t1 = (k + 1) * lo + min(k + 1, extra);
-				a.rangeBegin[br] = (int)(begin + (long long)t0 * a.tile);
-				a.rangeEnd[br] = (int)min((long long)end, begin + (long long)t1 * a.tile);
+				a.rangeBegin[br] = (int)max((long long)begin, base + (long long)t0 * a.tile);
+				a.rangeEnd[br] = (int)min((long long)end, base + (long long)t1 * a.tile);
 				a.rangeSeg[br] = s;
 				++br;
 			}
