@@ -53,8 +53,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="pairs_and24_32M",
-                   choices=sorted(workloads.WORKLOADS))
+                   choices=sorted(workloads.WORKLOADS) + ["served"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--requests", type=int, default=2000,
+                   help="served workload: number of requests")
+    p.add_argument("--server-budget", type=int, default=64,
+                   help="served workload: device memory budget in GiB")
     p.add_argument("--profile-only", action="store_true",
                    help="warm-up plus --steps sorts, no e2e/CPU legs (for ncu)")
     return p.parse_args()
@@ -173,10 +177,54 @@ def run_reference_segmented(args, case):
     return 0
 
 
+def run_reference_served(args):
+    """Reference arm for the served workload: the oracle's multithreaded LSD
+    sort (cpusort.cpp:122-186 restated) of each request in arrival order, over
+    a bounded sample of requests per step."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    sizes, has_values, end_bits, rng = served_requests(args.requests)
+    threads = os.cpu_count() or 1
+    take = max(1, int(np.searchsorted(np.cumsum(sizes), CPU_SAMPLE)))
+    pool = rng.integers(0, 1 << 32, int(sizes[:take].max()), dtype=np.uint64).astype(np.uint32)
+    idx = np.arange(pool.size, dtype=np.uint32)
+
+    def one_step():
+        t0 = time.perf_counter()
+        for i in range(take):
+            n, end = int(sizes[i]), int(end_bits[i])
+            p = (end + 7) // 8
+            widths = [end // p + (j < end % p) for j in range(p)]
+            vals = [idx[:n]] if has_values[i] else []
+            oracle.sort_lsd(pool[:n], vals, 1 if has_values[i] else 0, 0, widths, 1 << 15,
+                            threads)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        one_step()
+    times = [one_step() for _ in range(args.steps)]
+    elems = int(sizes[:take].sum())
+    value = elems * len(times) / sum(times) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(sum(times) / len(times) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "served_requests", "sample_requests": take,
+                       "sample": elems},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads,
+                             "kind": "port", "sample": f"first {take} requests per step"},
+            "e2e": {"value": round(value, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "served":
+        return run_reference_served(args)
     case = workloads.WORKLOADS[args.workload]()
     if isinstance(case, workloads.SegmentedCase):
         return run_reference_segmented(args, case)
@@ -509,6 +557,157 @@ def run_segmented(args, case, device, barrier, max_over_ranks, world, rank, loca
     return line
 
 
+def served_requests(count, seed=11):
+    """Served workload: sizes log-uniform in [1024, 16777216], half of the
+    requests keys-only and half key + one value, endBit uniform in {16, 24,
+    32}. Returns (sizes, has_values, end_bits, input offsets)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1024), np.log(16_777_216), count)).astype(np.int64)
+    has_values = rng.integers(0, 2, count).astype(bool)
+    end_bits = rng.choice([16, 24, 32], count)
+    return sizes, has_values, end_bits, rng
+
+
+def run_served(args, device, local):
+    """Served sort requests with Poisson arrivals: the sort server against
+    serial plain sortArray (one request at a time: copy in, sortArrayAsync,
+    copy out), at offered loads of 0.5x, 0.8x and 1.0x the serial capacity.
+    Latency is arrival (submission) to results in host memory."""
+    import threading
+    import torch
+    from mgpu_old_b200 import api
+
+    R = args.requests
+    sizes, has_values, end_bits, rng = served_requests(R)
+    # Input data: slices of one page-locked pool of random keys and values.
+    pool_n = 1 << 25
+    keys_pool = torch.from_numpy(rng.integers(0, 1 << 32, pool_n, dtype=np.uint64)
+                                 .astype(np.uint32).view(np.int32)).pin_memory()
+    vals_pool = torch.arange(pool_n, dtype=torch.int32).pin_memory()
+    starts = rng.integers(0, pool_n - sizes + 1)
+    # Outputs: a ring in page-locked memory (results are checked in the tests).
+    ring_n = 1 << 27
+    out_k = torch.empty(ring_n, dtype=torch.int32).pin_memory()
+    out_v = torch.empty(ring_n, dtype=torch.int32).pin_memory()
+    ring_at = (np.cumsum(sizes) - sizes) % (ring_n - int(sizes.max()))
+    total_elems = int(sizes.sum())
+    kptr, vptr = keys_pool.data_ptr(), vals_pool.data_ptr()
+    okp, ovp = out_k.data_ptr(), out_v.data_ptr()
+
+    # Serial baseline: one engine, one stream, device buffers for the largest
+    # request.
+    engine = api.MgpuSort()
+    nmax = int(sizes.max())
+    dk = [torch.empty(nmax, dtype=torch.int32, device=device) for _ in range(2)]
+    dv = [torch.empty(nmax, dtype=torch.int32, device=device) for _ in range(2)]
+    stream = torch.cuda.Stream(device)
+
+    def serial(arrivals):
+        lat = np.zeros(R)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for i in range(R):
+                now = time.perf_counter() - t0
+                if arrivals[i] > now:
+                    time.sleep(arrivals[i] - now)
+                n = int(sizes[i])
+                a = int(starts[i])
+                dk[0][:n].copy_(keys_pool[a:a + n], non_blocking=True)
+                d = api.SortData()
+                d.maxElements = d.numElements = n
+                d.firstBit, d.endBit = 0, int(end_bits[i])
+                d.keys[0], d.keys[1] = dk[0].data_ptr(), dk[1].data_ptr()
+                if has_values[i]:
+                    dv[0][:n].copy_(vals_pool[a:a + n], non_blocking=True)
+                    d.valueCount = 1
+                    d.values[0][0], d.values[0][1] = dv[0].data_ptr(), dv[1].data_ptr()
+                api.check(engine.sort_array_async(d, stream.cuda_stream))
+                o = int(ring_at[i])
+                res_k = dk[0] if d.keys[0] == dk[0].data_ptr() else dk[1]
+                out_k[o:o + n].copy_(res_k[:n], non_blocking=True)
+                if has_values[i]:
+                    res_v = dv[0] if d.values[0][0] == dv[0].data_ptr() else dv[1]
+                    out_v[o:o + n].copy_(res_v[:n], non_blocking=True)
+                stream.synchronize()
+                lat[i] = time.perf_counter() - t0 - arrivals[i]
+        span = time.perf_counter() - t0
+        return lat, span
+
+    def served(arrivals, server):
+        tickets = [None] * R
+        lat = np.zeros(R)
+        t0 = time.perf_counter()
+
+        def waiter():
+            for i in range(R):
+                while tickets[i] is None:
+                    time.sleep(0.0001)
+                st, lat[i] = server.wait(tickets[i])
+                api.check(st)
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        for i in range(R):
+            now = time.perf_counter() - t0
+            if arrivals[i] > now:
+                time.sleep(arrivals[i] - now)
+            n = int(sizes[i])
+            a = 4 * int(starts[i])
+            o = 4 * int(ring_at[i])
+            tickets[i] = server.submit(kptr + a, vptr + a if has_values[i] else None, n, 0,
+                                       int(end_bits[i]), okp + o,
+                                       ovp + o if has_values[i] else None)
+        th.join()
+        span = time.perf_counter() - t0
+        return lat, span
+
+    # Capacity of the serial path: all requests present at t = 0.
+    serial(np.zeros(R))                       # warm-up
+    lat0, span0 = serial(np.zeros(R))
+    capacity = R / span0                      # requests per second
+    server = api.SortServer(memory_budget=args.server_budget << 30, slots=4,
+                            coalesce_max=1 << 20)
+    served(np.zeros(R), server)               # warm-up: grows the memory pool
+    results = []
+    for load in (0.5, 0.8, 1.0):
+        rate = load * capacity
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, R))
+        sl, sspan = serial(arrivals)
+        vl, vspan = served(arrivals, server)
+        results.append({"offered_load": load, "rate_rps": round(rate, 1),
+                        "server": {"Mkeys_s": round(total_elems / vspan / 1e6, 1),
+                                   "p50_ms": round(float(np.percentile(vl, 50)) * 1e3, 3),
+                                   "p99_ms": round(float(np.percentile(vl, 99)) * 1e3, 3)},
+                        "serial_sortArray": {"Mkeys_s": round(total_elems / sspan / 1e6, 1),
+                                             "p50_ms": round(float(np.percentile(sl, 50)) * 1e3, 3),
+                                             "p99_ms": round(float(np.percentile(sl, 99)) * 1e3, 3)}})
+    # Saturation: everything at t = 0.
+    vl, vspan = served(np.zeros(R), server)
+    server.close()
+    engine.release()
+    best = total_elems / vspan / 1e6
+    line = {"metric": METRIC, "value": round(best, 1), "unit": UNIT, "n_gpus": 1,
+            "steps": R, "warmup": args.warmup, "ms_per_step": round(vspan / R * 1e3, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded numpy)",
+            "config": {"workload": "served_requests", "requests": R,
+                       "sizes": "log-uniform [1024, 16777216]",
+                       "mix": "50% keys-only / 50% key+value, endBit in {16, 24, 32}",
+                       "arrivals": "Poisson at 0.5/0.8/1.0 x serial capacity",
+                       "memory_budget_GiB": args.server_budget,
+                       "elements": total_elems, "parallelism": "replicas1"},
+            "e2e": {"value": round(best, 1), "unit": UNIT,
+                    "h2d_bytes_per_step": int(4 * (sizes + sizes * has_values).sum() / R),
+                    "d2h_bytes_per_step": int(4 * (sizes + sizes * has_values).sum() / R)},
+            "serial_capacity": {"requests_per_s": round(capacity, 1),
+                                "Mkeys_s": round(total_elems / span0 / 1e6, 1)},
+            "saturated_server": {"Mkeys_s": round(best, 1),
+                                 "p50_ms": round(float(np.percentile(vl, 50)) * 1e3, 3),
+                                 "p99_ms": round(float(np.percentile(vl, 99)) * 1e3, 3)},
+            "loads": results}
+    return line
+
+
 def ctypes_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -545,6 +744,11 @@ def main():
 
     from mgpu_old_b200 import api
     api.load_library()
+    if args.workload == "served":
+        line = run_served(args, device, local)
+        if rank == 0:
+            print(json.dumps(line))
+        return 0
     case = workloads.WORKLOADS[args.workload]()
     if isinstance(case, workloads.SegmentedCase):
         line = run_segmented(args, case, device, barrier, max_over_ranks, world, rank, local)
