@@ -11,8 +11,9 @@ copy and the flush are outside the timed region). `value` is device-resident
 throughput in Mkeys/s over the K timed steps (CUDA events on the sort's
 stream, max over ranks); `e2e` is the same metric through the C ABI with
 pinned host buffers, host->device and device->host copies inside the timed
-region. The roofline entry is the onesweep pass kernel, whose launches are
-timed with CUDA events inside the same timed steps (sortEnableKernelTiming).
+region. The roofline entry is the sort kernel of a pass (the dominant kernel),
+whose launches are timed with CUDA events inside the same timed steps
+(sortEnableKernelTiming).
 
 Multi-GPU: the sort path does not shard (one global order), so N ranks run N
 independent replicas of the workload ("weak" scaling); the only collectives
@@ -850,7 +851,7 @@ def main():
     e2e_ms = max_over_ranks(e2e_ms)
     e2e_value = case.n * world / (e2e_ms / args.steps * 1e-3) / 1e6
 
-    # Roofline of the onesweep pass kernel.
+    # Roofline of the sort kernel of a pass.
     peak, peak_src = hbm_peak()
     arrays = sorter.arrays
     pass_bytes = 2 * case.n * 4 * (1 + arrays)

@@ -5,8 +5,9 @@
 // management (:655-734), the LSD pass loop with ping-pong swaps and parity
 // (:541-601), sortArray / sortArrayEx argument handling (:607-648) and the
 // sortHost / sortDevice conveniences (:740-806). The per-pass kernel chain
-// (:356-530) is replaced by one upsweep launch per sort and one onesweep
-// launch per pass (sort_kernels.cu).
+// (:356-530) is replaced by three launches per pass (count, scan, sort over
+// a range partition; sort_kernels.cu), plus one upsweep per sort for
+// earlyExit.
 
 // The library is built with hidden visibility; the C ABI is all it exports.
 #pragma GCC visibility push(default)

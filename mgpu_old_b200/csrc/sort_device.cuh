@@ -1,6 +1,6 @@
 // Device-side building blocks shared by the sort kernels: PTX wrappers for
-// the mbarrier / bulk-copy (TMA) path, relaxed global loads and stores for
-// the decoupled lookback, and warp scans. sm_100a only.
+// the mbarrier / bulk-copy (TMA) path, relaxed and streaming global loads,
+// and warp scans. sm_100a only.
 #pragma once
 
 #include <cstdint>
@@ -9,9 +9,7 @@
 namespace mgpusort {
 
 // Error bits written to the device error word and to the host-mapped mirror.
-constexpr unsigned kErrLookbackTimeout = 1u;
 constexpr unsigned kErrBarrierTimeout = 2u;
-constexpr unsigned kErrQueueTimeout = 4u;
 constexpr unsigned kErrInjected = 8u;
 constexpr unsigned kErrBadSegments = 16u;
 
@@ -96,20 +94,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar,
 	while(!mbar_try_wait(bar, parity))
 		if(!budget.poll()) return false;
 	return true;
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(
-	const unsigned long long* p) {
-	unsigned long long v;
-	asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];"
-		: "=l"(v) : "l"(p) : "memory");
-	return v;
-}
-
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p,
-	unsigned long long v) {
-	asm volatile("st.relaxed.gpu.global.u64 [%0], %1;"
-		:: "l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {

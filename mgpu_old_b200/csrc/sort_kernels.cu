@@ -1,21 +1,25 @@
 // Radix sort kernels for sm_100a.
 //
-// A sort over the bit range [firstBit, endBit) runs as
-//   1. one upsweep launch that reads every key once and builds the digit
-//      histograms of all passes, then (last CTA) their exclusive scans;
-//   2. one onesweep launch per pass (least significant digit first). Each CTA
-//      takes the next tile id from an atomic counter, stages its tile of keys
-//      (and value arrays) in shared memory with bulk copies, ranks the keys
-//      stably by digit, finds the tile's global digit offsets with a
-//      decoupled lookback over the tiles before it, reorders the tile in
-//      shared memory into digit runs and writes each run contiguously.
+// A sort over the bit range [firstBit, endBit) runs one pass per digit,
+// least significant first. Each pass is three launches over a partition of
+// the array into R ranges of consecutive tiles (R = resident CTAs of the
+// sort kernel):
+//   1. count_kernel: each range's digit histogram (one read of the keys);
+//   2. scan_kernel: per digit, the exclusive prefix over ranges and the
+//      digit's total;
+//   3. sort_kernel: CTA r starts every digit at (keys with smaller digits in
+//      the whole array) + (keys with this digit in ranges before r) and
+//      walks its tiles in order: bulk-copy the tile into shared memory, rank
+//      its keys stably by digit, reorder it into digit runs, store each run
+//      contiguously, advance the digit offsets. No tile waits for another.
+// With earlyExit an upsweep launch first builds every pass's histogram in one
+// read so that single-digit passes can be skipped.
 //
 // This replaces the reference's per-pass count / hist1 / hist2 / hist3 / sort
 // kernel chain (sort/src/mgpusort/mgpusort.cpp:421-516; kernels
-// sort/src/kernels/count.cu, hist1.cu, hist2.cu, hist3.cu, sort.cu) with two
-// kernels and one read of the keys for all counting. The ordering contract is
-// the same: every pass is a stable partition by its digit, so the passes
-// compose into a stable sort by the whole bit field.
+// sort/src/kernels/count.cu, hist1.cu, hist2.cu, hist3.cu, sort.cu). The
+// ordering contract is the same: every pass is a stable partition by its
+// digit, so the passes compose into a stable sort by the whole bit field.
 
 #include "sort_kernels.h"
 #include "sort_device.cuh"

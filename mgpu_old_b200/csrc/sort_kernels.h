@@ -17,17 +17,15 @@ constexpr int kDigitBins = 256;
 // Device control block, one per engine. The upsweep adds every key's digits
 // into hist, and its last CTA turns hist into the exclusive offsets, sets
 // trivial[p] when pass p has a single non-empty digit, and zeroes hist and
-// ticket again. Each pass kernel draws tile ids from tileCounter[p]; the CTA
-// that draws the last id re-arms the counter. So the block is clean after
-// every complete sort and needs a memset only after an error.
+// ticket again. So the block is clean after every complete sort and needs a
+// memset only after an error (the error word).
 struct Control {
 	unsigned hist[kMaxBins];
 	unsigned offsets[kMaxBins];
 	unsigned trivial[kMaxPasses];
-	unsigned tileCounter[kMaxPasses];
 	unsigned ticket;
 	unsigned error;
-	unsigned reserved[62];
+	unsigned reserved[94];
 };
 
 // Digit layout of a sort: pass p sorts by bits [shift[p], shift[p] +
