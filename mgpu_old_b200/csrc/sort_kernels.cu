@@ -235,19 +235,35 @@ __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a)
 		// aligned.
 		const uint4* src = reinterpret_cast<const uint4*>(a.keys + begin);
 		const int nvec = (int)((end - begin) / 4);
+		// Software pipelined: the next U loads are in flight while the
+		// current U are counted.
 		constexpr int U = 4;
 		int i = tid;
-		for(; i + (U - 1) * kCountThreads < nvec; i += U * kCountThreads) {
-			uint4 q[U];
+		uint4 q[U];
+		bool have = i + (U - 1) * kCountThreads < nvec;
+		if(have) {
 #pragma unroll
 			for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + i + u * kCountThreads);
+		}
+		while(have) {
+			uint4 cur[U];
+#pragma unroll
+			for(int u = 0; u < U; ++u) cur[u] = q[u];
+			const int inext = i + U * kCountThreads;
+			const bool haveNext = inext + (U - 1) * kCountThreads < nvec;
+			if(haveNext) {
+#pragma unroll
+				for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + inext + u * kCountThreads);
+			}
 #pragma unroll
 			for(int u = 0; u < U; ++u) {
-				add(q[u].x);
-				add(q[u].y);
-				add(q[u].z);
-				add(q[u].w);
+				add(cur[u].x);
+				add(cur[u].y);
+				add(cur[u].z);
+				add(cur[u].w);
 			}
+			i = inext;
+			have = haveNext;
 		}
 		for(; i < nvec; i += kCountThreads) {
 			const uint4 q = ld_stream_u4(src + i);
@@ -278,21 +294,28 @@ struct ScanArgs {
 	int numRanges;
 };
 
-// One warp per digit: exclusive scan of the digit's range counts.
-__global__ void __launch_bounds__(256) scan_kernel(const ScanArgs a) {
-	const int lane = threadIdx.x & 31;
-	const int d = blockIdx.x * 8 + (threadIdx.x >> 5);
-	const unsigned* in = a.rangeCounts + (size_t)d * a.numRanges;
-	unsigned* out = a.rangeOffsets + (size_t)d * a.numRanges;
-	unsigned carry = 0;
-	for(int base = 0; base < a.numRanges; base += 32) {
-		const int r = base + lane;
-		const unsigned v = r < a.numRanges ? in[r] : 0u;
-		const unsigned incl = warp_inclusive_scan(v, lane);
-		if(r < a.numRanges) out[r] = carry + incl - v;
-		carry += __shfl_sync(0xffffffffu, incl, 31);
+// One CTA per digit, one thread per range (R <= kMaxRanges = 1024): the
+// exclusive scan of the digit's range counts and the digit's total.
+__global__ void __launch_bounds__(1024) scan_kernel(const ScanArgs a) {
+	__shared__ unsigned sWarp[32];
+	const int d = blockIdx.x;
+	const int t = threadIdx.x;
+	const int lane = t & 31;
+	const int warp = t >> 5;
+	const int R = a.numRanges;
+	const unsigned v = t < R ? a.rangeCounts[(size_t)d * R + t] : 0u;
+	const unsigned incl = warp_inclusive_scan(v, lane);
+	if(lane == 31) sWarp[warp] = incl;
+	__syncthreads();
+	if(warp == 0) {
+		const int nw = blockDim.x >> 5;
+		const unsigned w = lane < nw ? sWarp[lane] : 0u;
+		const unsigned wi = warp_inclusive_scan(w, lane);
+		sWarp[lane] = wi - w;
+		if(lane == 31) a.totals[d] = wi;
 	}
-	if(lane == 0) a.totals[d] = carry;
+	__syncthreads();
+	if(t < R) a.rangeOffsets[(size_t)d * R + t] = sWarp[warp] + incl - v;
 }
 
 struct SortArgs {
@@ -310,13 +333,16 @@ struct SortArgs {
 };
 
 // Tile shapes measured on B200 (sort kernel time over 32 Mi and 64 Mi
-// key-value pairs and 16 Mi keys with six value arrays, 256..512 threads x
-// 12..32 keys): larger tiles give each digit longer runs per tile, so fewer
-// partially written sectors reach DRAM; 384 x 20 was best for keys, indices
-// and one value array, 512 x 14 for several value arrays.
+// key-value pairs, 256..512 threads x 12..32 keys): larger tiles give each
+// digit longer runs per tile, so fewer partially written sectors reach DRAM;
+// 384 x 20 was best for keys, indices and one value array (256 x 20 with
+// three CTAs per SM was 2% faster at 32 Mi skewed keys but 29% slower at
+// 64 Mi uniform keys). Several value arrays keep a destination and a source
+// position per key in registers: 384 x 16 is the largest shape without
+// spills at two CTAs per SM.
 template<int VM> struct SortConfig {
-	static constexpr int kThreads = VM >= 2 ? 512 : 384;
-	static constexpr int kItems = VM >= 2 ? 14 : 20;
+	static constexpr int kThreads = 384;
+	static constexpr int kItems = VM >= 2 ? 16 : 20;
 	static constexpr int kMinBlocks = 2;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
@@ -459,30 +485,108 @@ __device__ __forceinline__ void sort_setup(const SortSmem<VM>& sm) {
 	for(int i = threadIdx.x; i < L::NW * kDigitBins; i += L::NT) sm.warpHist[i] = 0;
 }
 
-// Identity pass over [begin, end) (every key has the same digit).
+// Identity pass over [begin, end) (every key has the same digit): a
+// streaming copy of the keys and value arrays (index mode: the positions).
+// With 16-byte aligned buffers the aligned middle moves in 16-byte vectors,
+// every array's load of a step in flight before its stores.
 template<int VM>
 __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 	long long end, long long indexBase) {
 	constexpr int NV = SortLayout<VM>::NV;
-	for(long long i = begin + threadIdx.x; i < end; i += SortLayout<VM>::NT) {
+	constexpr int NT = SortLayout<VM>::NT;
+	auto copy_one = [&](long long i) {
 		a.buf.keysOut[i] = a.buf.keysIn[i];
 		if constexpr(VM == kValueIndex) a.buf.valsOut[0][i] = (unsigned)(i - indexBase);
 #pragma unroll
 		for(int v = 0; v < NV; ++v) a.buf.valsOut[v][i] = a.buf.valsIn[v][i];
+	};
+	long long head = end;
+	long long vecEnd = end;
+	if(a.useBulk) {
+		head = min(end, (begin + 3) & ~3ll);
+		vecEnd = head + ((end - head) & ~3ll);
+	}
+	for(long long i = begin + threadIdx.x; i < head; i += NT) copy_one(i);
+	if(head < vecEnd) {
+		const long long v0 = head >> 2;
+		const long long nvec = (vecEnd - head) >> 2;
+		for(long long j = threadIdx.x; j < nvec; j += NT) {
+			const long long e = (v0 + j) << 2;
+			uint4 k = ld_stream_u4(reinterpret_cast<const uint4*>(a.buf.keysIn) + v0 + j);
+			uint4 vals[NV > 0 ? NV : 1];
+#pragma unroll
+			for(int v = 0; v < NV; ++v)
+				vals[v] = ld_stream_u4(reinterpret_cast<const uint4*>(a.buf.valsIn[v]) + v0 + j);
+			reinterpret_cast<uint4*>(a.buf.keysOut)[v0 + j] = k;
+			if constexpr(VM == kValueIndex) {
+				const unsigned x = (unsigned)(e - indexBase);
+				reinterpret_cast<uint4*>(a.buf.valsOut[0])[v0 + j] =
+					make_uint4(x, x + 1, x + 2, x + 3);
+			}
+#pragma unroll
+			for(int v = 0; v < NV; ++v)
+				reinterpret_cast<uint4*>(a.buf.valsOut[v])[v0 + j] = vals[v];
+		}
+	}
+	for(long long i = vecEnd + threadIdx.x; i < end; i += NT) copy_one(i);
+}
+
+// Once the warps of a tile have counted their digits (sm.warpHist): per
+// digit the tile's count and exclusive start, and for every warp the position
+// where its run of the digit begins in the reordered tile (digit start +
+// counts of the warps before it), written over the warp counts. Element p of
+// the reordered tile then belongs at scatter[digit] + p globally, and each
+// digit's running offset advances by the tile's real count (padding is only
+// ever in digit 255 and is not counted). One barrier inside; the caller
+// synchronizes before reading the results.
+template<int VM>
+__device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int count) {
+	using L = SortLayout<VM>;
+	constexpr int NW = L::NW;
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const int warp = tid >> 5;
+	unsigned c[NW];
+	unsigned tileTotal = 0;
+	if(tid < kDigitBins) {
+#pragma unroll
+		for(int w = 0; w < NW; ++w) {
+			c[w] = sm.warpHist[w * kDigitBins + tid];
+			tileTotal += c[w];
+		}
+	}
+	const unsigned incl = warp_inclusive_scan(tileTotal, lane);
+	if(lane == 31 && tid < kDigitBins) sm.scan[warp] = incl;
+	__syncthreads();
+	if(tid < kDigitBins) {
+		unsigned prefix = 0;
+		for(int w = 0; w < warp; ++w) prefix += sm.scan[w];
+		const unsigned digStart = prefix + incl - tileTotal;
+		unsigned run = digStart;
+#pragma unroll
+		for(int w = 0; w < NW; ++w) {
+			sm.warpHist[w * kDigitBins + tid] = run;
+			run += c[w];
+		}
+		const unsigned mine = tileTotal - (tid == kDigitBins - 1 ? L::TILE - count : 0);
+		const unsigned g = sm.running[tid];
+		sm.scatter[tid] = (int)(g - digStart);
+		sm.running[tid] = g + mine;
 	}
 }
 
 // Sort the tiles of [begin, end) in order, from digit offsets already in
 // sm.running (element p of digit d's run in a tile goes to running[d] + p,
-// then running[d] advances by the tile's count). Each tile: stable warp
-// ranks, digit starts, reorder into digit runs in shared memory, run-wise
-// stores; value arrays past the first stream through one buffer. The next
-// tile's keys are copied in while a tile is sorted (two key slots), its
-// first value array as soon as this tile has stored its own. Index mode
-// writes position - indexBase. Requires sort_setup and a barrier before.
+// then running[d] advances by the tile's count). Keys only, index mode or
+// one value array. Each tile: stable warp ranks, digit starts, reorder into
+// digit runs in shared memory, run-wise stores. The next tile's keys are
+// copied in while a tile is sorted (two key slots), its value array as soon
+// as this tile has stored its own. Index mode writes position - indexBase.
+// Requires sort_setup and a barrier before.
 template<int VM, bool BYTE>
-__device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
+__device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 	long long begin, long long end, long long indexBase, unsigned& phase) {
+	static_assert(VM <= 1, "one value array at most");
 
 	using L = SortLayout<VM>;
 	constexpr int NT = L::NT;
@@ -494,11 +598,8 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 	constexpr unsigned kTileBytes = TILE * 4;
 
 	unsigned* sVals = sm.vals;
-	unsigned* sStream = sm.stream;
 	unsigned* sWarpHist = sm.warpHist;
-	unsigned* sRunning = sm.running;
 	int* sScatter = sm.scatter;
-	unsigned* sScan = sm.scan;
 	uint64_t* sBar = sm.bar;
 
 	const int tid = threadIdx.x;
@@ -562,38 +663,7 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 		}
 		__syncthreads();
 
-		// Per digit: the tile's count, its exclusive digit start, and for every
-		// warp the position where its run of the digit begins in the reordered
-		// tile (digit start + counts of the warps before it).
-		unsigned c[NW];
-		unsigned tileTotal = 0;
-		if(tid < kDigitBins) {
-#pragma unroll
-			for(int w = 0; w < NW; ++w) {
-				c[w] = sWarpHist[w * kDigitBins + tid];
-				tileTotal += c[w];
-			}
-		}
-		const unsigned incl = warp_inclusive_scan(tileTotal, lane);
-		if(lane == 31 && tid < kDigitBins) sScan[warp] = incl;
-		__syncthreads();
-		if(tid < kDigitBins) {
-			unsigned prefix = 0;
-			for(int w = 0; w < warp; ++w) prefix += sScan[w];
-			const unsigned digStart = prefix + incl - tileTotal;
-			unsigned run = digStart;
-#pragma unroll
-			for(int w = 0; w < NW; ++w) {
-				sWarpHist[w * kDigitBins + tid] = run;
-				run += c[w];
-			}
-			// Global position of element p of digit tid's run: scatter + p.
-			// Padding is only ever in digit 255 and is not counted.
-			const unsigned mine = tileTotal - (tid == kDigitBins - 1 ? TILE - count : 0);
-			const unsigned g = sRunning[tid];
-			sScatter[tid] = (int)(g - digStart);
-			sRunning[tid] = g + mine;
-		}
+		tile_digit_starts<VM>(sm, count);
 
 		// Every warp's keys leave shared memory for registers before the tile
 		// is reordered in place.
@@ -627,13 +697,6 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 #pragma unroll
 			for(int i = 0; i < IPT; ++i) sVals[rank[i]] = vals[i];
 		}
-		if constexpr(NV >= 2) {
-			// The second value array heads for the stream buffer now.
-			if(bulk && tid == 0) {
-				fence_proxy_async_smem();
-				stage_tile(sStream, a.buf.valsIn[1] + tileStart, kTileBytes, &sBar[3]);
-			}
-		}
 		if(a.failTile >= 0 && tileStart / TILE == a.failTile && tid == 0) {
 			// Injected fault (tests only): wait on a barrier that nothing
 			// completes, so the bounded wait runs out and is reported.
@@ -666,46 +729,6 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 			}
 		}
 
-		// Value arrays 2..V: array v arrives in the stream buffer (requested
-		// while array v - 1 was reordered), is read out, array v + 1 is
-		// requested into the stream buffer, and array v is reordered in the
-		// value buffer and stored.
-#pragma unroll
-		for(int v = 1; v < NV; ++v) {
-			unsigned vals[IPT];
-			if(bulk) {
-				if(!mbar_wait_bounded(&sBar[3], (phase >> 3) & 1u))
-					report_error(a.devError, a.hostError, kErrBarrierTimeout);
-				phase ^= 1u << 3;
-#pragma unroll
-				for(int i = 0; i < IPT; ++i) vals[i] = sStream[warpBase + i * 32 + lane];
-			} else {
-#pragma unroll
-				for(int i = 0; i < IPT; ++i) {
-					const int idx = warpBase + i * 32 + lane;
-					vals[i] = idx < count ? a.buf.valsIn[v][tileStart + idx] : 0u;
-				}
-			}
-			// Everyone has read the stream buffer and finished the stores
-			// that read the value buffer.
-			__syncthreads();
-			if(bulk && tid == 0 && v + 1 < NV) {
-				fence_proxy_async_smem();
-				stage_tile(sStream, a.buf.valsIn[v + 1] + tileStart, kTileBytes, &sBar[3]);
-			}
-#pragma unroll
-			for(int i = 0; i < IPT; ++i) sVals[rank[i]] = vals[i];
-			__syncthreads();
-#pragma unroll
-			for(int j = 0; j < IPT; ++j) {
-				const int p = j * NT + tid;
-				if(p < count) {
-					const int dst = sScatter[digit(sKeys[p])] + p;
-					a.buf.valsOut[v][dst] = sVals[p];
-				}
-			}
-		}
-
 		for(int i = tid; i < NW * kDigitBins; i += NT) sWarpHist[i] = 0;
 		__syncthreads();
 
@@ -720,6 +743,176 @@ __device__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 		slot = KSLOTS == 2 ? slot ^ 1 : 0;
 		tileStart = next;
 	}
+}
+
+// The same range sort with two or more value arrays. Keys are ranked and
+// reordered as above; the reorder also records, for every position of the
+// reordered tile, the element's position in the input tile. Each thread then
+// holds, for its IPT output positions, the global destination and the source
+// position in registers, and every value array is staged with one bulk copy
+// and written straight from its staging buffer: valsOut[v][dst] =
+// staged[src]. Two staging buffers alternate, so array v + 1 is in flight
+// while array v is written; the next tile's keys are requested as soon as
+// this tile's keys are stored. Tiles without bulk copies gather their values
+// from global memory (a window of one tile).
+template<int VM, bool BYTE>
+__device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
+	long long begin, long long end, unsigned& phase) {
+
+	using L = SortLayout<VM>;
+	constexpr int NT = L::NT;
+	constexpr int IPT = L::IPT;
+	constexpr int TILE = L::TILE;
+	constexpr int NV = L::NV;
+	constexpr unsigned kTileBytes = TILE * 4;
+	static_assert(NV >= 2 && L::KSLOTS == 1, "multi-array layout");
+
+	unsigned* sKeys = sm.keys(0);
+	// Staging buffer 0 (mbarrier 3) takes the even arrays and is free while
+	// the keys are ranked; buffer 1 (mbarrier 2) holds the source positions
+	// until they are read, then the odd arrays.
+	unsigned* sBuf0 = sm.stream;
+	unsigned* sBuf1 = sm.vals;
+	unsigned* sWarpHist = sm.warpHist;
+	int* sScatter = sm.scatter;
+	uint64_t* sBar = sm.bar;
+
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
+	const int warp = tid >> 5;
+	const int warpBase = warp * 32 * IPT;
+
+	auto tile_is_bulk = [&](long long t) {
+		return a.useBulk && (t & 3) == 0 && t + TILE <= end;
+	};
+	auto wait_bar = [&](int b) {
+		if(!mbar_wait_bounded(&sBar[b], (phase >> b) & 1u))
+			report_error(a.devError, a.hostError, kErrBarrierTimeout);
+		phase ^= 1u << b;
+	};
+
+	if(tid == 0 && begin < end && tile_is_bulk(begin)) {
+		fence_proxy_async_smem();
+		stage_tile(sKeys, a.buf.keysIn + begin, kTileBytes, &sBar[0]);
+		stage_tile(sBuf0, a.buf.valsIn[0] + begin, kTileBytes, &sBar[3]);
+	}
+
+	const DigitOf<BYTE> digit(a.shift, a.width);
+	const unsigned ltMask = lanemask_lt();
+	unsigned nClear[4];
+#pragma unroll
+	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
+
+	for(long long tileStart = begin; tileStart < end;) {
+		const long long next = (tileStart & ~3ll) + TILE;
+		const int count = (int)(min(next, end) - tileStart);
+		const bool bulk = tile_is_bulk(tileStart);
+		const bool nextBulk = next < end && tile_is_bulk(next);
+
+		unsigned* myHist = sWarpHist + warp * kDigitBins;
+		unsigned rank[IPT];
+		if(bulk) {
+			wait_bar(0);
+			rank_tile<IPT, true, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+				ltMask, nClear, rank);
+		} else {
+			for(int i = tid; i < TILE; i += NT)
+				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
+			__syncthreads();
+			rank_tile<IPT, false, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+				ltMask, nClear, rank);
+		}
+		__syncthreads();
+		tile_digit_starts<VM>(sm, count);
+
+		unsigned keys[IPT];
+#pragma unroll
+		for(int i = 0; i < IPT; ++i) keys[i] = sKeys[warpBase + i * 32 + lane];
+		__syncthreads();
+
+		// Reorder the keys in place; record each element's input position.
+#pragma unroll
+		for(int i = 0; i < IPT; ++i) {
+			const unsigned pos = (rank[i] & 0xffffu)
+				+ sWarpHist[warp * kDigitBins + (rank[i] >> 16)];
+			sKeys[pos] = keys[i];
+			sBuf1[pos] = (unsigned)(warpBase + i * 32 + lane);
+		}
+		if(a.failTile >= 0 && tileStart / TILE == a.failTile && tid == 0) {
+			// Injected fault (tests only): wait on a barrier that nothing
+			// completes, so the bounded wait runs out and is reported.
+			if(!mbar_wait_bounded(&sBar[5], 0))
+				report_error(a.devError, a.hostError, kErrInjected);
+		}
+		__syncthreads();
+
+		// Destinations and sources of this thread's output positions; the
+		// keys are stored run-wise.
+		int dst[IPT];
+		unsigned src[IPT];
+#pragma unroll
+		for(int j = 0; j < IPT; ++j) {
+			const int p = j * NT + tid;
+			dst[j] = -1;
+			src[j] = 0;
+			if(p < count) {
+				const unsigned k = sKeys[p];
+				dst[j] = sScatter[digit(k)] + p;
+				src[j] = sBuf1[p];
+				a.buf.keysOut[dst[j]] = k;
+			}
+		}
+		for(int i = tid; i < L::NW * kDigitBins; i += NT) sWarpHist[i] = 0;
+		__syncthreads();
+
+		// The key buffer and buffer 1 are free: the next tile's keys and this
+		// tile's second value array head there.
+		if(tid == 0) {
+			fence_proxy_async_smem();
+			if(nextBulk) stage_tile(sKeys, a.buf.keysIn + next, kTileBytes, &sBar[0]);
+			if(bulk) stage_tile(sBuf1, a.buf.valsIn[1] + tileStart, kTileBytes, &sBar[2]);
+		}
+
+#pragma unroll
+		for(int v = 0; v < NV; ++v) {
+			unsigned* buf = (v & 1) ? sBuf1 : sBuf0;
+			if(bulk) {
+				wait_bar((v & 1) ? 2 : 3);
+#pragma unroll
+				for(int j = 0; j < IPT; ++j)
+					if(dst[j] >= 0) a.buf.valsOut[v][dst[j]] = buf[src[j]];
+			} else {
+				const unsigned* in = a.buf.valsIn[v] + tileStart;
+#pragma unroll
+				for(int j = 0; j < IPT; ++j)
+					if(dst[j] >= 0) a.buf.valsOut[v][dst[j]] = in[src[j]];
+			}
+			if(v + 2 < NV) {
+				// Everyone has read the buffer: array v + 2 goes into it.
+				__syncthreads();
+				if(bulk && tid == 0) {
+					fence_proxy_async_smem();
+					stage_tile(buf, a.buf.valsIn[v + 2] + tileStart, kTileBytes,
+						&sBar[(v & 1) ? 2 : 3]);
+				}
+			}
+		}
+		__syncthreads();
+
+		// Buffer 0 is free: the next tile's first value array.
+		if(tid == 0 && nextBulk) {
+			fence_proxy_async_smem();
+			stage_tile(sBuf0, a.buf.valsIn[0] + next, kTileBytes, &sBar[3]);
+		}
+		tileStart = next;
+	}
+}
+
+template<int VM, bool BYTE>
+__device__ __forceinline__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
+	long long begin, long long end, long long indexBase, unsigned& phase) {
+	if constexpr(VM >= 2) sort_range_multi<VM, BYTE>(a, sm, begin, end, phase);
+	else sort_range_single<VM, BYTE>(a, sm, begin, end, indexBase, phase);
 }
 
 // One pass over a whole array: CTA r sorts range r of the split.
@@ -1270,7 +1463,7 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	s.rangeOffsets = scratch + (size_t)kDigitBins * kMaxRanges;
 	s.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
 	s.numRanges = split.numRanges;
-	scan_kernel<<<kDigitBins / 8, 256, 0, stream>>>(s);
+	scan_kernel<<<kDigitBins, (split.numRanges + 31) / 32 * 32, 0, stream>>>(s);
 	return cudaGetLastError();
 }
 
