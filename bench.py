@@ -54,8 +54,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="pairs_and24_32M",
-                   choices=sorted(workloads.WORKLOADS) + ["served"])
+                   choices=sorted(workloads.WORKLOADS) + ["served", "bwt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--bwt-bytes", type=int, default=8 << 20,
+                   help="bwt workload: block size in bytes")
+    p.add_argument("--bwt-key", type=int, default=16,
+                   help="bwt workload: gpuKeySize (symbols ordered on the GPU)")
     p.add_argument("--requests", type=int, default=2000,
                    help="served workload: number of requests")
     p.add_argument("--server-budget", type=int, default=64,
@@ -87,6 +91,115 @@ def workload_config(case, args, extra=None):
 def _plan(case):
     from mgpu_old_b200 import api
     return api.plan_passes(case.first_bit, case.end_bit)
+
+
+# ---------------------------------------------------------------------------
+# The BWT caller (include/mgpubwt.h): block sort of an English-like text block.
+
+BWT_METRIC = "bwtSortBlock MB/s"
+BWT_CPU_SAMPLE = 1 << 20
+
+
+def bwt_config(args, extra=None):
+    cfg = {"workload": "bwt_text", "block_bytes": args.bwt_bytes, "gpu_key_size": args.bwt_key,
+           "block": "seeded English-like text (500-word Zipf vocabulary)",
+           "parallelism": f"replicas{args.gpus}"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def cpu_bwt_sample(block):
+    """Seconds of one host block sort of `block`: the reference BWT library's
+    own string quicksort (bwt/src/mgpubwt/cpusort.cpp, built in oracle/_ref)
+    when present, else the oracle's stable sort of rotations."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    t0 = time.perf_counter()
+    if oracle.ref_bwt_lib() is not None:
+        oracle.ref_bwt_block(block)
+        kind = "reference"
+    else:
+        oracle.bwt(block, 1)
+        kind = "port"
+    return time.perf_counter() - t0, kind
+
+
+def cpu_baseline_bwt(args, budget_s=10.0):
+    block = workloads.text_block(min(args.bwt_bytes, BWT_CPU_SAMPLE))
+    total_t, reps, kind = 0.0, 0, "port"
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or reps == 0:
+        t, kind = cpu_bwt_sample(block)
+        total_t += t
+        reps += 1
+    what = ("the reference's QSortStrings (bwt/src/mgpubwt/cpusort.cpp) over every rotation"
+            if kind == "reference" else "the oracle's stable sort of rotations")
+    return {"value": round(block.size * reps / total_t / 1e6, 3), "unit": "MB/s", "cores": 1,
+            "kind": kind, "sample": f"{block.size}-byte block of the same text, {what}, "
+                                    f"1 thread, {reps} repetitions"}
+
+
+def run_bwt(args, barrier, max_over_ranks, world, rank):
+    """bwtSortBlock on a host block (its API takes and returns host memory),
+    wall clock around each synchronous call; every result is checked against
+    the oracle's rotation sort once."""
+    from mgpu_old_b200 import api
+    from oracle import oracle
+    block = workloads.text_block(args.bwt_bytes)
+    eng = api.BwtEngine()
+    for _ in range(max(args.warmup, 3)):
+        st, idx, xf, seg, av = eng.sort_block(block, args.bwt_key)
+        if st != api.BwtStatus.SUCCESS:
+            raise SystemExit(f"bwtSortBlock: {api.bwt_status_string(st)}")
+    e_idx, e_xf, e_seg, _ = oracle.bwt(block, args.bwt_key)
+    if not (np.array_equal(idx, e_idx) and np.array_equal(xf, e_xf) and seg == e_seg):
+        raise SystemExit("bwt result differs from the oracle")
+    barrier()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        eng.sort_block(block, args.bwt_key)
+        times.append(time.perf_counter() - t0)
+    ms = max_over_ranks(sum(times) / len(times) * 1e3)
+    value = block.size * world / (ms * 1e-3) / 1e6
+    eng.close()
+    line = {"metric": BWT_METRIC, "value": round(value, 2), "unit": "MB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded numpy)",
+            "config": bwt_config(args, {"tie_groups": seg, "mean_tie_group": round(av, 3),
+                                        "timing": "wall clock around the synchronous host call"}),
+            "e2e": {"value": round(value, 2), "unit": "MB/s",
+                    "h2d_bytes_per_step": 2 * block.size + 32,
+                    "d2h_bytes_per_step": 5 * block.size}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_bwt(args)
+    return line
+
+
+def run_reference_bwt(args):
+    """Reference arm for the BWT caller: the reference's host block sort
+    (QSortStrings over every rotation, as its TinyBlockSort) on a bounded
+    1 MiB block of the same text per step."""
+    block = workloads.text_block(min(args.bwt_bytes, BWT_CPU_SAMPLE))
+    for _ in range(args.warmup):
+        cpu_bwt_sample(block)
+    runs = [cpu_bwt_sample(block) for _ in range(args.steps)]
+    total = sum(t for t, _ in runs)
+    kind = runs[-1][1]
+    value = block.size * len(runs) / total / 1e6
+    line = {"impl": "reference", "metric": BWT_METRIC, "value": round(value, 3), "unit": "MB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total / len(runs) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": bwt_config(args, {"sample_bytes": block.size}),
+            "cpu_baseline": {"value": round(value, 3), "unit": "MB/s", "cores": 1, "kind": kind,
+                             "sample": f"{block.size}-byte block per step"},
+            "e2e": {"value": round(value, 3), "unit": "MB/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
 
 
 # ---------------------------------------------------------------------------
@@ -226,6 +339,8 @@ def run_reference(args):
         return 0
     if args.workload == "served":
         return run_reference_served(args)
+    if args.workload == "bwt":
+        return run_reference_bwt(args)
     case = workloads.WORKLOADS[args.workload]()
     if isinstance(case, workloads.SegmentedCase):
         return run_reference_segmented(args, case)
@@ -747,6 +862,14 @@ def main():
     api.load_library()
     if args.workload == "served":
         line = run_served(args, device, local)
+        if rank == 0:
+            print(json.dumps(line))
+        return 0
+    if args.workload == "bwt":
+        line = run_bwt(args, barrier, max_over_ranks, world, rank)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
         if rank == 0:
             print(json.dumps(line))
         return 0

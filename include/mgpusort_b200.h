@@ -50,6 +50,33 @@ sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable);
 sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches);
 
+/* Key types of sortArrayTyped. */
+typedef enum {
+	SORT_KEY_UINT32 = 0,
+	SORT_KEY_INT32 = 1,
+	SORT_KEY_FLOAT32 = 2
+} sortKeyType_t;
+
+/* sortArrayAsync for signed or floating-point keys: keys[0] holds int32 or
+ * IEEE-754 binary32 bit patterns (keyType, a sortKeyType_t) and the sort
+ * orders them numerically, floats in the total order of their sign-magnitude
+ * image: -NaN < -inf < ... < -0.0 < +0.0 < ... < +inf < +NaN. The keys are
+ * mapped in place to that order-preserving uint32 image before the first
+ * pass and back after the last (the transform of the reference's
+ * sort/src/kernels/common.cu:159-186), so they come out as the caller's bit
+ * patterns; [firstBit, endBit) selects bits of the image. No counterpart in
+ * the reference's sort API. An unknown keyType is SORT_STATUS_INVALID_VALUE. */
+sortStatus_t SORTAPI sortArrayTyped(sortEngine_t engine, sortData_t data,
+	int keyType, CUstream stream);
+
+/* The k-th smallest key by sorting: sortArray on data, then element k of
+ * the sorted keys copied to *value (waits for the sort). This is the
+ * sort-based selection of the reference's select benchmark
+ * (select/src/selecttest/mgpusorttest.cpp:3-32), kept as one call. k outside
+ * [0, numElements) or a null value is SORT_STATUS_INVALID_VALUE. */
+sortStatus_t SORTAPI sortSelectKey(sortEngine_t engine, sortData_t data, int k,
+	unsigned int* value);
+
 /* Batched segmented sort: sort each of numSegments independent segments of
  * the array described by `data` stably by its bit field, in one call. No
  * counterpart in the reference, whose callers sort many arrays with one

@@ -77,9 +77,14 @@ EXPORTED_SYMBOLS = (
     # mgpusort_b200.h (no reference counterpart)
     "sortArrayAsync", "sortSynchronize", "sortPlanPasses", "sortInjectFault",
     "sortEnableKernelTiming", "sortReadKernelTiming", "sortArrayNoAlloc",
-    "sortSegmentedArray", "sortServerCreate", "sortServerSubmit", "sortServerPoll",
+    "sortSegmentedArray", "sortArrayTyped", "sortSelectKey", "sortServerCreate", "sortServerSubmit", "sortServerPoll",
     "sortServerWait", "sortServerDestroy",
+    # mgpubwt.h (inc/mgpubwt.h, bwt/src/mgpubwt/bwt.def)
+    "bwtStatusString", "bwtCreateEngine", "bwtDestroyEngine", "bwtSortBlock",
 )
+
+# sortKeyType_t of sortArrayTyped.
+KEY_UINT32, KEY_INT32, KEY_FLOAT32 = 0, 1, 2
 
 # Largest numElements accepted by sortArrayNoAlloc (SORT_NOALLOC_MAX_ELEMENTS).
 NOALLOC_MAX_ELEMENTS = 4194304
@@ -121,12 +126,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                          POINTER(ctypes.c_double), POINTER(c_int)]),
         "sortArrayNoAlloc": (c_int, [data_t, c_void_p]),
         "sortSegmentedArray": (c_int, [engine_t, data_t, c_void_p, c_int, c_void_p]),
+        "sortArrayTyped": (c_int, [engine_t, data_t, c_int, c_void_p]),
+        "sortSelectKey": (c_int, [engine_t, data_t, c_int, POINTER(c_uint)]),
         "sortServerCreate": (c_int, [POINTER(ServerConfig), POINTER(c_void_p)]),
         "sortServerSubmit": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                      c_void_p, c_void_p, POINTER(ctypes.c_ulonglong)]),
         "sortServerPoll": (c_int, [c_void_p, ctypes.c_ulonglong, POINTER(c_int)]),
         "sortServerWait": (c_int, [c_void_p, ctypes.c_ulonglong, POINTER(ctypes.c_double)]),
         "sortServerDestroy": (c_int, [c_void_p]),
+        "bwtStatusString": (c_char_p, [c_int]),
+        "bwtCreateEngine": (c_int, [c_char_p, POINTER(c_void_p)]),
+        "bwtDestroyEngine": (c_int, [c_void_p]),
+        "bwtSortBlock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, POINTER(c_int),
+                                 POINTER(c_int), POINTER(ctypes.c_float)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -200,6 +212,18 @@ class MgpuSort:
     def sort_array_async(self, data: SortData, stream: int) -> int:
         return load_library().sortArrayAsync(self._engine, ctypes.byref(data),
                                              c_void_p(stream))
+
+    def sort_array_typed(self, data: SortData, key_type: int, stream: int = 0) -> int:
+        """sortArrayTyped: KEY_INT32 / KEY_FLOAT32 keys (KEY_UINT32 = plain)."""
+        return load_library().sortArrayTyped(self._engine, ctypes.byref(data), int(key_type),
+                                             c_void_p(stream))
+
+    def select_key(self, data: SortData, k: int) -> tuple[int, int]:
+        """sortSelectKey: (status, k-th smallest key after sorting data)."""
+        v = c_uint(0)
+        st = load_library().sortSelectKey(self._engine, ctypes.byref(data), int(k),
+                                          ctypes.byref(v))
+        return st, int(v.value)
 
     def synchronize(self) -> int:
         return load_library().sortSynchronize(self._engine)
@@ -327,3 +351,64 @@ class MgpuSortData(SortData):
         load_library().sortFreeData(ctypes.byref(self))
         self._attached_keys = [False, False]
         self._attached_vals = [[False, False] for _ in range(6)]
+
+
+class BwtStatus(enum.IntEnum):
+    """bwtStatus_t, in the order of inc/mgpubwt.h:21-34."""
+    SUCCESS = 0
+    NOT_INITIALIZED = 1
+    DEVICE_ALLOC_FAILED = 2
+    INVALID_CONTEXT = 3
+    KERNEL_NOT_FOUND = 4
+    KERNEL_ERROR = 5
+    LAUNCH_ERROR = 6
+    INVALID_VALUE = 7
+    DEVICE_ERROR = 8
+    NOT_IMPLEMENTED = 9
+    UNSUPPORTED_DEVICE = 10
+    SORT_ERROR = 11
+
+
+def bwt_status_string(status: int) -> str | None:
+    s = load_library().bwtStatusString(int(status))
+    return s.decode() if s is not None else None
+
+
+class BwtEngine:
+    """bwtCreateEngine / bwtSortBlock / bwtDestroyEngine (inc/mgpubwt.h)."""
+
+    def __init__(self, kernel_path: str = ""):
+        lib = load_library()
+        handle = c_void_p()
+        st = lib.bwtCreateEngine(kernel_path.encode(), ctypes.byref(handle))
+        if st != BwtStatus.SUCCESS:
+            raise RuntimeError(bwt_status_string(st) or f"status {st}")
+        self._engine = handle
+
+    def sort_block(self, block, key_size: int):
+        """Returns (status, indices int32[n], transform uint8[n], segCount,
+        avSegSize) for the bytes of `block` (bytes or a uint8 array)."""
+        import numpy as np
+        data = np.frombuffer(bytes(block), dtype=np.uint8) if not hasattr(block, "dtype") \
+            else np.ascontiguousarray(block, dtype=np.uint8)
+        n = int(data.size)
+        indices = np.zeros(max(n, 1), dtype=np.int32)
+        transform = np.zeros(max(n, 1), dtype=np.uint8)
+        seg = c_int(-1)
+        av = ctypes.c_float(-1.0)
+        st = load_library().bwtSortBlock(
+            self._engine, data.ctypes.data_as(c_void_p), n, int(key_size),
+            transform.ctypes.data_as(c_void_p), indices.ctypes.data_as(POINTER(c_int)),
+            ctypes.byref(seg), ctypes.byref(av))
+        return int(st), indices[:n], transform[:n], seg.value, av.value
+
+    def close(self) -> None:
+        if self._engine:
+            load_library().bwtDestroyEngine(self._engine)
+            self._engine = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

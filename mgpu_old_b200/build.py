@@ -22,6 +22,7 @@ SOURCES = [
     "sort_kernels.cu",
     "noalloc.cu",
     "server.cpp",
+    "bwt.cu",
 ]
 
 NVCC_FLAGS = [

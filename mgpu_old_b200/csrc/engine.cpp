@@ -199,9 +199,11 @@ void swap_buffers(sortData_d* d) {
 }
 
 // The whole sort of one sortData_d: validation, upsweep, the pass loop.
-// bitPass 0 selects sortArray's plan, 1..6 sortArrayEx's.
+// bitPass 0 selects sortArray's plan, 1..6 sortArrayEx's. Signed and float
+// keys (keyType) are mapped to their uint32 image in place before the first
+// pass and back after the last.
 sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
-	cudaStream_t stream) {
+	cudaStream_t stream, int keyType = mgpusort::kKeyUint32) {
 	if(!e || !d) return SORT_STATUS_INVALID_VALUE;
 	sortStatus_t pending = take_device_error(e);
 	if(pending != SORT_STATUS_SUCCESS) return pending;
@@ -232,6 +234,10 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 		e->dirty = false;
 	}
 
+	cudaError_t ce = mgpusort::launch_key_transform(
+		reinterpret_cast<unsigned*>(d->keys[0]), n, keyType, true, stream);
+	if(ce != cudaSuccess) return launch_status(ce);
+
 	bool bulk = true;
 	for(int i = 0; i < 2; ++i) bulk = bulk && aligned16(d->keys[i]);
 	for(int i = 0; i < numArrays; ++i)
@@ -244,7 +250,6 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 	// pass runs as a straight copy.
 	bool skip[mgpusort::kMaxPasses] = {};
 	int slot = -1;
-	cudaError_t ce = cudaSuccess;
 	if(d->earlyExit) {
 		slot = timing_begin(e, kTimedUpsweep, stream);
 		ce = mgpusort::launch_upsweep(
@@ -293,6 +298,9 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 			stream);
 		if(ce != cudaSuccess) return launch_status(ce);
 	}
+	ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(d->keys[0]), n,
+		keyType, false, stream);
+	if(ce != cudaSuccess) return launch_status(ce);
 	cudaEventRecord(e->done, stream);
 	return SORT_STATUS_SUCCESS;
 }
@@ -583,6 +591,28 @@ sortStatus_t SORTAPI sortArrayEx(sortEngine_t engine, sortData_t data,
 sortStatus_t SORTAPI sortArrayAsync(sortEngine_t engine, sortData_t data,
 	CUstream stream) {
 	return sort_impl(engine, data, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+sortStatus_t SORTAPI sortArrayTyped(sortEngine_t engine, sortData_t data,
+	int keyType, CUstream stream) {
+	if(keyType != mgpusort::kKeyUint32 && keyType != mgpusort::kKeyInt32 &&
+		keyType != mgpusort::kKeyFloat32) return SORT_STATUS_INVALID_VALUE;
+	return sort_impl(engine, data, 0, reinterpret_cast<cudaStream_t>(stream), keyType);
+}
+
+sortStatus_t SORTAPI sortSelectKey(sortEngine_t engine, sortData_t data, int k,
+	unsigned int* value) {
+	if(!engine || !data || !value || k < 0 || k >= data->numElements)
+		return SORT_STATUS_INVALID_VALUE;
+	sortStatus_t st = sort_impl(engine, data, 0, cudaStreamLegacy);
+	if(st != SORT_STATUS_SUCCESS) return st;
+	const unsigned* keys = reinterpret_cast<const unsigned*>(data->keys[0]);
+	if(cudaMemcpy(value, keys + k, sizeof(unsigned), cudaMemcpyDeviceToHost)
+		!= cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_DEVICE_ERROR;
+	}
+	return take_device_error(engine);
 }
 
 sortStatus_t SORTAPI sortSegmentedArray(sortEngine_t engine, sortData_t data,

@@ -1698,4 +1698,31 @@ cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream) {
 	return cudaGetLastError();
 }
 
+// Order-preserving uint32 image of signed and float keys (the transform of
+// the reference's sort/src/kernels/common.cu:159-186, written from its
+// definition): int32 flips the sign bit; float32 flips the sign bit of
+// non-negative values and every bit of negative ones, so unsigned order is
+// -NaN < -inf < ... < -0.0 < +0.0 < ... < +inf < +NaN. The inverse undoes
+// it: an image with the top bit set came from a non-negative value.
+__global__ void key_transform_kernel(unsigned* keys, int n, int keyType, int forward) {
+	for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+		i += (long long)gridDim.x * blockDim.x) {
+		unsigned k = keys[i];
+		if(keyType == kKeyInt32) k ^= 0x80000000u;
+		else {
+			const bool top = (k >> 31) != 0;
+			k ^= (forward ? top : !top) ? 0xffffffffu : 0x80000000u;
+		}
+		keys[i] = k;
+	}
+}
+
+cudaError_t launch_key_transform(unsigned* keys, int n, int keyType, bool forward,
+	cudaStream_t stream) {
+	if(n <= 0 || keyType == kKeyUint32) return cudaSuccess;
+	int grid = (int)std::min<long long>(((long long)n + 255) / 256, 4096);
+	key_transform_kernel<<<grid, 256, 0, stream>>>(keys, n, keyType, forward ? 1 : 0);
+	return cudaGetLastError();
+}
+
 } // namespace mgpusort

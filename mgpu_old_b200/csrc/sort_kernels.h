@@ -119,4 +119,13 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream);
 
+// Key types with an order-preserving uint32 image (sortArrayTyped).
+constexpr int kKeyUint32 = 0;
+constexpr int kKeyInt32 = 1;
+constexpr int kKeyFloat32 = 2;
+
+// Maps n keys in place to their uint32 radix image (forward) or back.
+cudaError_t launch_key_transform(unsigned* keys, int n, int keyType, bool forward,
+	cudaStream_t stream);
+
 } // namespace mgpusort

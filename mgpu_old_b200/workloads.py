@@ -108,6 +108,28 @@ def keys_uniform32_64m() -> SortCase:
     return c
 
 
+def text_block(n: int, seed: int = 7) -> np.ndarray:
+    """Seeded English-like bytes for the BWT block sort: words from a
+    generated 500-word vocabulary (1-8 letters, letter order by English
+    frequency) drawn with Zipf(1.3) frequencies, separated by spaces and, one
+    time in 12, newlines. Stands in for the reference's text test block."""
+    rng = np.random.default_rng(seed)
+    letters = np.frombuffer(b"etaoinshrdlcumwfgypbvkjxqz", dtype=np.uint8)
+    vocab = [bytes(letters[rng.integers(0, 26, int(rng.integers(1, 9)))].tolist())
+             for _ in range(500)]
+    picks = np.minimum(rng.zipf(1.3, size=n // 2 + 16), 500) - 1
+    seps = rng.random(picks.size) < 1 / 12
+    out = bytearray()
+    for w, nl in zip(picks, seps):
+        out += vocab[int(w)]
+        out += b"\n" if nl else b" "
+        if len(out) >= n:
+            break
+    while len(out) < n:
+        out += out[:n - len(out)]
+    return np.frombuffer(bytes(out[:n]), dtype=np.uint8).copy()
+
+
 WORKLOADS = {
     "keys_u32_1M": keys_uniform32,
     "pairs_and24_32M": pairs_and24,

@@ -228,4 +228,53 @@ int oracle_reference_ex_plan(int numBits, int bitPass, int* widths) {
 	return passes;
 }
 
+// Burrows-Wheeler block sort of a cyclic block, what bwtSortBlock computes
+// (bwt/src/mgpubwt/mgpubwt.cpp:213-371): indices[i] = start of the i-th
+// smallest rotation (rotations equal as whole strings in start order),
+// transform[i] = block[(indices[i] + count - 1) % count]. segCount /
+// avSegSize: the groups of two or more rotations that share their first
+// keySize symbols, and their mean size; blocks under 3000 bytes are sorted
+// on the host by the reference and report one group of count
+// (mgpubwt.cpp:180-205). Returns 0, or -1 for invalid arguments.
+int oracle_bwt(const uint8_t* block, int count, int keySize, int* indices,
+	uint8_t* transform, int* segCount, float* avSegSize) {
+	if(count < 0 || keySize < 1 || keySize > 24) return -1;
+	std::vector<uint8_t> sym(2 * (size_t)count + 1);
+	if(count) {
+		std::memcpy(sym.data(), block, count);
+		std::memcpy(sym.data() + count, block, count);
+	}
+	std::vector<int> order(count);
+	std::iota(order.begin(), order.end(), 0);
+	std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+		return std::memcmp(sym.data() + a, sym.data() + b, count) < 0;
+	});
+	int groups = 0;
+	long long grouped = 0;
+	if(count < 3000) {
+		groups = count ? 1 : 0;
+		grouped = count;
+	} else {
+		int start = 0;
+		for(int i = 1; i <= count; ++i) {
+			const bool head = i == count ||
+				std::memcmp(sym.data() + order[i - 1], sym.data() + order[i], keySize) != 0;
+			if(!head) continue;
+			if(i - start >= 2) {
+				++groups;
+				grouped += i - start;
+			}
+			start = i;
+		}
+	}
+	for(int i = 0; i < count; ++i) {
+		indices[i] = order[i];
+		transform[i] = sym[(size_t)order[i] + count - 1];
+	}
+	*segCount = groups;
+	*avSegSize = count < 3000 ? (float)count
+		: (groups ? (float)((double)grouped / groups) : 0.0f);
+	return 0;
+}
+
 } // extern "C"

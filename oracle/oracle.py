@@ -1,5 +1,6 @@
 """ctypes binding of liboracle.so (oracle.cpp) and of the reference's own CPU
-radix sort built into _ref/ (ref_cpusort_shim.cpp). TEST INFRASTRUCTURE ONLY.
+code built into _ref/: its radix sort demo (ref_cpusort_shim.cpp) and its BWT
+library's string quicksort (ref_bwt_shim.cpp). TEST INFRASTRUCTURE ONLY.
 """
 from __future__ import annotations
 
@@ -13,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_cpusort.so")
+REF_BWT_LIB = os.path.join(HERE, "_ref", "libref_bwt.so")
 REFERENCE_TREE = "/root/reference"
 
 _u32p = POINTER(c_uint)
@@ -28,6 +30,7 @@ def build(ref: bool = True) -> None:
 
 _lib = None
 _ref = None
+_ref_bwt = None
 
 
 def lib() -> ctypes.CDLL:
@@ -49,6 +52,9 @@ def lib() -> ctypes.CDLL:
         l.oracle_std_sort_keys.argtypes = [_u32p, c_int]
         l.oracle_reference_ex_plan.restype = c_int
         l.oracle_reference_ex_plan.argtypes = [c_int, c_int, POINTER(c_int)]
+        l.oracle_bwt.restype = c_int
+        l.oracle_bwt.argtypes = [c_void_p, c_int, c_int, POINTER(c_int), c_void_p,
+                                 POINTER(c_int), POINTER(ctypes.c_float)]
         _lib = l
     return _lib
 
@@ -138,3 +144,52 @@ def std_sort_keys(keys: np.ndarray) -> np.ndarray:
     out = np.array(keys, dtype=np.uint32, copy=True)
     lib().oracle_std_sort_keys(_p(out), out.size)
     return out
+
+
+def bwt(block, key_size: int):
+    """(indices, transform, segCount, avSegSize) of the block's rotations
+    (oracle_bwt)."""
+    data = np.frombuffer(bytes(block), dtype=np.uint8) if not hasattr(block, "dtype") \
+        else np.ascontiguousarray(block, dtype=np.uint8)
+    n = int(data.size)
+    idx = np.zeros(max(n, 1), dtype=np.int32)
+    xf = np.zeros(max(n, 1), dtype=np.uint8)
+    seg = c_int(0)
+    av = ctypes.c_float(0)
+    rc = lib().oracle_bwt(data.ctypes.data_as(c_void_p), n, int(key_size),
+                          idx.ctypes.data_as(POINTER(c_int)), xf.ctypes.data_as(c_void_p),
+                          ctypes.byref(seg), ctypes.byref(av))
+    if rc:
+        raise ValueError("oracle_bwt: invalid arguments")
+    return idx[:n], xf[:n], seg.value, av.value
+
+
+def ref_bwt_lib() -> ctypes.CDLL | None:
+    """The reference BWT library's cpusort.cpp built here, or None."""
+    global _ref_bwt
+    if _ref_bwt is None and os.path.exists(REF_BWT_LIB):
+        r = ctypes.CDLL(REF_BWT_LIB)
+        r.ref_bwt_qsort_strings.restype = None
+        r.ref_bwt_qsort_strings.argtypes = [POINTER(c_int), POINTER(c_int), c_void_p, c_int]
+        _ref_bwt = r
+    return _ref_bwt
+
+
+def ref_bwt_block(block):
+    """Rotation order and transform of a block by the reference's own host
+    block sort: QSortStrings over every rotation of the doubled block, as its
+    TinyBlockSort does (bwt/src/mgpubwt/mgpubwt.cpp:180-205)."""
+    r = ref_bwt_lib()
+    if r is None:
+        return None
+    data = np.ascontiguousarray(np.frombuffer(bytes(block), dtype=np.uint8)
+                                if not hasattr(block, "dtype") else block, dtype=np.uint8)
+    n = int(data.size)
+    sym = np.concatenate([data, data])
+    idx = np.arange(n, dtype=np.int32)
+    if n >= 2:
+        base = idx.ctypes.data_as(POINTER(c_int))
+        last = ctypes.cast(ctypes.addressof(base.contents) + 4 * (n - 1), POINTER(c_int))
+        r.ref_bwt_qsort_strings(base, last, sym.ctypes.data_as(c_void_p), n)
+    xf = sym[(idx.astype(np.int64) + n - 1)]
+    return idx, xf

@@ -18,9 +18,7 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"\b(\w+)\s+SORTAPI\s+(\w+)\s*\(", text):
-            names.add(m.group(2))
-        for m in re.finditer(r"\bSORTAPI\s+(\w+)\s*\(", text):
+        for m in re.finditer(r"\b(?:SORTAPI|BWTAPI)\s+(\w+)\s*\(", text):
             names.add(m.group(1))
     return names
 
@@ -115,3 +113,36 @@ def test_create_engine_without_a_device_fails_cleanly(lib):
     st = lib.sortCreateEngine(b"", ctypes.byref(h))
     assert st in (api.SortStatus.INVALID_CONTEXT, api.SortStatus.UNSUPPORTED_DEVICE)
     assert not h.value
+
+
+def test_bwt_status_strings(lib):
+    from mgpu_old_b200 import api
+    for s in api.BwtStatus:
+        assert api.bwt_status_string(s) == "BWT_STATUS_" + s.name
+    assert api.bwt_status_string(12) is None
+    assert api.bwt_status_string(-1) is None
+
+
+@pytest.mark.skipif(HAVE_GPU, reason="checks the no-device error path")
+def test_bwt_create_engine_without_gpu(lib):
+    from mgpu_old_b200 import api
+    handle = ctypes.c_void_p()
+    st = lib.bwtCreateEngine(b"", ctypes.byref(handle))
+    assert st != api.BwtStatus.SUCCESS
+    assert not handle.value
+
+
+def test_bwt_host_only_block_without_engine(lib, oracle_mod):
+    """Blocks under 3000 bytes are sorted on the host; no engine is needed
+    (mgpubwt.cpp:217-221)."""
+    import numpy as np
+    blk = np.frombuffer(b"abracadabra", dtype=np.uint8).copy()
+    idx = (ctypes.c_int * 11)()
+    xf = (ctypes.c_ubyte * 11)()
+    seg, av = ctypes.c_int(), ctypes.c_float()
+    st = lib.bwtSortBlock(None, blk.ctypes.data_as(ctypes.c_void_p), 11, 4, xf, idx,
+                          ctypes.byref(seg), ctypes.byref(av))
+    assert st == 0
+    assert bytes(xf) == b"rdarcaaaabb"
+    e_idx, _, e_seg, e_av = oracle_mod.bwt(blk, 4)
+    assert list(idx) == list(e_idx) and seg.value == e_seg and av.value == e_av
