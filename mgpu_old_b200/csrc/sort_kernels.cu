@@ -28,6 +28,37 @@
 
 namespace mgpusort {
 
+// Programmatic dependent launch: the count, scan and sort kernels of the
+// passes are launched so that each may be scheduled while its predecessor
+// in the stream drains. Each waits (griddepcontrol.wait) for the
+// predecessor to complete, with its memory visible, before touching global
+// memory, and then lets its own successor launch. Launched without the
+// attribute (or after a non-kernel stream operation) the wait returns at
+// once.
+__device__ __forceinline__ void wait_for_predecessor() {
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void allow_successor() {
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template<typename Arg>
+static cudaError_t launch_dependent(void (*kernel)(Arg), int grid, int block,
+	size_t smem, cudaStream_t stream, const Arg& arg) {
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(block);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = stream;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, kernel, arg);
+}
+
 ////////////////////////////////////////////////////////////////////////////////
 // Upsweep: digit histograms of every pass in one read of the keys.
 
@@ -215,6 +246,8 @@ struct CountArgs {
 // and lanes never share a counter (warps do, through the atomic).
 __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a) {
 	__shared__ unsigned sHist[kDigitBins * 32];
+	wait_for_predecessor();
+	allow_successor();
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int r = blockIdx.x;
@@ -298,6 +331,8 @@ struct ScanArgs {
 // exclusive scan of the digit's range counts and the digit's total.
 __global__ void __launch_bounds__(1024) scan_kernel(const ScanArgs a) {
 	__shared__ unsigned sWarp[32];
+	wait_for_predecessor();
+	allow_successor();
 	const int d = blockIdx.x;
 	const int t = threadIdx.x;
 	const int lane = t & 31;
@@ -921,6 +956,8 @@ __global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks
 sort_kernel(const SortArgs a) {
 	using L = SortLayout<VM>;
 	extern __shared__ __align__(128) unsigned smem[];
+	wait_for_predecessor();
+	allow_successor();
 	const SortSmem<VM> sm(smem);
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
@@ -1456,24 +1493,27 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
 	c.split = split;
 	c.rangeCounts = rangeCounts;
-	count_kernel<<<split.numRanges, kCountThreads, 0, stream>>>(c);
+	cudaError_t e = launch_dependent(count_kernel, split.numRanges, kCountThreads, 0,
+		stream, c);
+	if(e != cudaSuccess) return e;
 
 	ScanArgs s;
 	s.rangeCounts = rangeCounts;
 	s.rangeOffsets = scratch + (size_t)kDigitBins * kMaxRanges;
 	s.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
 	s.numRanges = split.numRanges;
-	scan_kernel<<<kDigitBins, (split.numRanges + 31) / 32 * 32, 0, stream>>>(s);
-	return cudaGetLastError();
+	return launch_dependent(scan_kernel, kDigitBins, (split.numRanges + 31) / 32 * 32, 0,
+		stream, s);
 }
 
 template<int VM>
-static void launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
+static cudaError_t launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
 	using L = SortLayout<VM>;
 	if(a.width == 8 && (a.shift & 7) == 0)
-		sort_kernel<VM, true><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
-	else
-		sort_kernel<VM, false><<<a.split.numRanges, L::NT, L::kBytes, stream>>>(a);
+		return launch_dependent(sort_kernel<VM, true>, a.split.numRanges, L::NT, L::kBytes,
+			stream, a);
+	return launch_dependent(sort_kernel<VM, false>, a.split.numRanges, L::NT, L::kBytes,
+		stream, a);
 }
 
 cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
@@ -1493,17 +1533,16 @@ cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
 	a.useBulk = useBulk ? 1 : 0;
 	a.failTile = failTile;
 	switch(valueMode) {
-		case -1: launch_sort_vm<-1>(a, stream); break;
-		case 0: launch_sort_vm<0>(a, stream); break;
-		case 1: launch_sort_vm<1>(a, stream); break;
-		case 2: launch_sort_vm<2>(a, stream); break;
-		case 3: launch_sort_vm<3>(a, stream); break;
-		case 4: launch_sort_vm<4>(a, stream); break;
-		case 5: launch_sort_vm<5>(a, stream); break;
-		case 6: launch_sort_vm<6>(a, stream); break;
+		case -1: return launch_sort_vm<-1>(a, stream);
+		case 0: return launch_sort_vm<0>(a, stream);
+		case 1: return launch_sort_vm<1>(a, stream);
+		case 2: return launch_sort_vm<2>(a, stream);
+		case 3: return launch_sort_vm<3>(a, stream);
+		case 4: return launch_sort_vm<4>(a, stream);
+		case 5: return launch_sort_vm<5>(a, stream);
+		case 6: return launch_sort_vm<6>(a, stream);
 		default: return cudaErrorInvalidValue;
 	}
-	return cudaGetLastError();
 }
 
 cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
