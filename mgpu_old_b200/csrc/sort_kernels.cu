@@ -372,13 +372,15 @@ struct SortArgs {
 // digit longer runs per tile, so fewer partially written sectors reach DRAM;
 // 384 x 20 was best for keys, indices and one value array (256 x 20 with
 // three CTAs per SM was 2% faster at 32 Mi skewed keys but 29% slower at
-// 64 Mi uniform keys). Several value arrays keep a destination and a source
-// position per key in registers: 384 x 16 is the largest shape without
-// spills at two CTAs per SM.
+// 64 Mi uniform keys: more ranges, more write fronts). Several value arrays
+// multiply the write fronts (ranges x digits x arrays), and a front is
+// revisited only once per tile of its range, so partial sectors leave L2
+// before they are completed: one CTA of 768 x 8 per SM halves the ranges and
+// was 1.21x faster than two of 384 x 16 at 16 Mi keys with six arrays.
 template<int VM> struct SortConfig {
-	static constexpr int kThreads = 384;
-	static constexpr int kItems = VM >= 2 ? 16 : 20;
-	static constexpr int kMinBlocks = 2;
+	static constexpr int kThreads = VM >= 2 ? 768 : 384;
+	static constexpr int kItems = VM >= 2 ? 8 : 20;
+	static constexpr int kMinBlocks = VM >= 2 ? 1 : 2;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
