@@ -835,41 +835,22 @@ def main():
         return run_reference(args)
 
     import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=device)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from mgpu_old_b200 import replicas
+    reps = replicas.from_env("nccl")
+    world, rank, local, device = reps.world, reps.rank, reps.local, reps.device
+    barrier, max_over_ranks = reps.barrier, reps.max_over_ranks
 
     from mgpu_old_b200 import api
     api.load_library()
     if args.workload == "served":
         line = run_served(args, device, local)
+        reps.close()
         if rank == 0:
             print(json.dumps(line))
         return 0
     if args.workload == "bwt":
         line = run_bwt(args, barrier, max_over_ranks, world, rank)
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
+        reps.close()
         if rank == 0:
             print(json.dumps(line))
         return 0
@@ -878,9 +859,7 @@ def main():
         line = run_segmented(args, case, device, barrier, max_over_ranks, world, rank, local)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_segmented(case)
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
+        reps.close()
         if rank == 0:
             print(json.dumps(line))
         return 0
@@ -1058,9 +1037,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(case)
     engine.release()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
