@@ -377,6 +377,10 @@ struct SortArgs {
 // revisited only once per tile of its range, so partial sectors leave L2
 // before they are completed: one CTA of 768 x 8 per SM halves the ranges and
 // was 1.21x faster than two of 384 x 16 at 16 Mi keys with six arrays.
+// mbarriers of a sort CTA: keys, up to six value arrays, the fault wait.
+constexpr int kNumBars = 8;
+constexpr int kFaultBar = 7;
+
 template<int VM> struct SortConfig {
 	static constexpr int kThreads = VM >= 2 ? 768 : 384;
 	static constexpr int kItems = VM >= 2 ? 8 : 20;
@@ -393,23 +397,21 @@ template<int VM> struct SortLayout {
 	static constexpr int NW = NT / 32;
 	static constexpr int KSLOTS = SortConfig<VM>::kKeySlots;
 	static constexpr int NV = VM > 0 ? VM : 0;
-	// One value buffer holds the first value array (or the generated
-	// indices); with more arrays, each further one is copied into the stream
-	// buffer while the one before it is reordered in the value buffer.
-	static constexpr int NVBUF = VM == 0 ? 0 : 1;
-	static constexpr int NSTREAM = NV >= 2 ? 1 : 0;
+	// Keys only: no value buffer. One value array (or the generated
+	// indices): one buffer, reordered in place. Two or more: a buffer of
+	// source positions, then one staging buffer per value array.
+	static constexpr int NVBUF = VM == 0 ? 0 : (NV >= 2 ? 1 + NV : 1);
 	// Word offsets into dynamic shared memory.
 	static constexpr int kKeys = 0;
 	static constexpr int kVals = kKeys + KSLOTS * TILE;
-	static constexpr int kStream = kVals + NVBUF * TILE;
-	static constexpr int kWarpHist = kStream + NSTREAM * TILE;
+	static constexpr int kWarpHist = kVals + NVBUF * TILE;
 	static constexpr int kDigStart = kWarpHist + NW * kDigitBins;
 	static constexpr int kCount = kDigStart + kDigitBins;
 	static constexpr int kRunning = kCount + kDigitBins;
 	static constexpr int kScatter = kRunning + kDigitBins;
 	static constexpr int kScan = kScatter + kDigitBins;
 	static constexpr int kBar = kScan + 32;          // 8-byte aligned: even
-	static constexpr int kWords = kBar + 2 * 6;       // 6 mbarriers
+	static constexpr int kWords = kBar + 2 * kNumBars;
 	static constexpr size_t kBytes = sizeof(unsigned) * kWords;
 	static_assert(kBar % 2 == 0, "mbarriers need 8-byte alignment");
 	static_assert(TILE < 65536, "ranks are packed in 16 bits");
@@ -493,21 +495,26 @@ template<int VM> struct SortSmem {
 	using L = SortLayout<VM>;
 	unsigned* smem;
 	unsigned* vals;
-	unsigned* stream;
 	unsigned* warpHist;
 	unsigned* running;
 	int* scatter;
 	unsigned* scan;
-	// mbarriers: [0..1] key slots, [2] value buffer, [3] stream buffer,
-	// [5] injected-fault wait (never completed).
+	// mbarriers: one key slot: [0] keys, [1 + v] value array v; two key
+	// slots: [0..1] keys, [2] value buffer. [kFaultBar] is the injected-fault
+	// wait (never completed).
 	uint64_t* bar;
 	__device__ __forceinline__ explicit SortSmem(unsigned* base)
-		: smem(base), vals(base + L::kVals), stream(base + L::kStream),
+		: smem(base), vals(base + L::kVals),
 		  warpHist(base + L::kWarpHist), running(base + L::kRunning),
 		  scatter(reinterpret_cast<int*>(base + L::kScatter)), scan(base + L::kScan),
 		  bar(reinterpret_cast<uint64_t*>(base + L::kBar)) { }
 	__device__ __forceinline__ unsigned* keys(int slot) const {
 		return smem + L::kKeys + slot * L::TILE;
+	}
+	// Several value arrays: the source positions and staging buffer v.
+	__device__ __forceinline__ unsigned* positions() const { return vals; }
+	__device__ __forceinline__ unsigned* staged(int v) const {
+		return vals + (1 + v) * L::TILE;
 	}
 };
 
@@ -516,7 +523,7 @@ template<int VM>
 __device__ __forceinline__ void sort_setup(const SortSmem<VM>& sm) {
 	using L = SortLayout<VM>;
 	if(threadIdx.x == 0) {
-		for(int i = 0; i < 6; ++i) mbar_init(&sm.bar[i], 1);
+		for(int i = 0; i < kNumBars; ++i) mbar_init(&sm.bar[i], 1);
 		fence_mbar_init();
 	}
 	for(int i = threadIdx.x; i < L::NW * kDigitBins; i += L::NT) sm.warpHist[i] = 0;
@@ -737,7 +744,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 		if(a.failTile >= 0 && tileStart / TILE == a.failTile && tid == 0) {
 			// Injected fault (tests only): wait on a barrier that nothing
 			// completes, so the bounded wait runs out and is reported.
-			if(!mbar_wait_bounded(&sBar[5], 0))
+			if(!mbar_wait_bounded(&sBar[kFaultBar], 0))
 				report_error(a.devError, a.hostError, kErrInjected);
 		}
 		__syncthreads();
@@ -786,12 +793,14 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 // reordered as above; the reorder also records, for every position of the
 // reordered tile, the element's position in the input tile. Each thread then
 // holds, for its IPT output positions, the global destination and the source
-// position in registers, and every value array is staged with one bulk copy
-// and written straight from its staging buffer: valsOut[v][dst] =
-// staged[src]. Two staging buffers alternate, so array v + 1 is in flight
-// while array v is written; the next tile's keys are requested as soon as
-// this tile's keys are stored. Tiles without bulk copies gather their values
-// from global memory (a window of one tile).
+// position in registers, and every value array is written straight from its
+// staging buffer: valsOut[v][dst] = staged_v[src]. Each array has its own
+// staging buffer, so all of a tile's arrays are in flight at once: they are
+// requested as soon as the previous tile has written its own (the first
+// tile's with its keys) and arrive while the keys are ranked. The next
+// tile's keys are requested as soon as this tile's keys are stored. Tiles
+// without bulk copies gather their values from global memory (a window of
+// one tile).
 template<int VM, bool BYTE>
 __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 	long long begin, long long end, unsigned& phase) {
@@ -802,14 +811,10 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 	constexpr int TILE = L::TILE;
 	constexpr int NV = L::NV;
 	constexpr unsigned kTileBytes = TILE * 4;
-	static_assert(NV >= 2 && L::KSLOTS == 1, "multi-array layout");
+	static_assert(NV >= 2 && NV < kFaultBar && L::KSLOTS == 1, "multi-array layout");
 
 	unsigned* sKeys = sm.keys(0);
-	// Staging buffer 0 (mbarrier 3) takes the even arrays and is free while
-	// the keys are ranked; buffer 1 (mbarrier 2) holds the source positions
-	// until they are read, then the odd arrays.
-	unsigned* sBuf0 = sm.stream;
-	unsigned* sBuf1 = sm.vals;
+	unsigned* sPos = sm.positions();
 	unsigned* sWarpHist = sm.warpHist;
 	int* sScatter = sm.scatter;
 	uint64_t* sBar = sm.bar;
@@ -827,11 +832,17 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 			report_error(a.devError, a.hostError, kErrBarrierTimeout);
 		phase ^= 1u << b;
 	};
+	// Value array v of the tile at t into staging buffer v (mbarrier 1 + v).
+	auto stage_values = [&](long long t) {
+#pragma unroll
+		for(int v = 0; v < NV; ++v)
+			stage_tile(sm.staged(v), a.buf.valsIn[v] + t, kTileBytes, &sBar[1 + v]);
+	};
 
 	if(tid == 0 && begin < end && tile_is_bulk(begin)) {
 		fence_proxy_async_smem();
 		stage_tile(sKeys, a.buf.keysIn + begin, kTileBytes, &sBar[0]);
-		stage_tile(sBuf0, a.buf.valsIn[0] + begin, kTileBytes, &sBar[3]);
+		stage_values(begin);
 	}
 
 	const DigitOf<BYTE> digit(a.shift, a.width);
@@ -873,12 +884,12 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 			const unsigned pos = (rank[i] & 0xffffu)
 				+ sWarpHist[warp * kDigitBins + (rank[i] >> 16)];
 			sKeys[pos] = keys[i];
-			sBuf1[pos] = (unsigned)(warpBase + i * 32 + lane);
+			sPos[pos] = (unsigned)(warpBase + i * 32 + lane);
 		}
 		if(a.failTile >= 0 && tileStart / TILE == a.failTile && tid == 0) {
 			// Injected fault (tests only): wait on a barrier that nothing
 			// completes, so the bounded wait runs out and is reported.
-			if(!mbar_wait_bounded(&sBar[5], 0))
+			if(!mbar_wait_bounded(&sBar[kFaultBar], 0))
 				report_error(a.devError, a.hostError, kErrInjected);
 		}
 		__syncthreads();
@@ -895,26 +906,24 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 			if(p < count) {
 				const unsigned k = sKeys[p];
 				dst[j] = sScatter[digit(k)] + p;
-				src[j] = sBuf1[p];
+				src[j] = sPos[p];
 				a.buf.keysOut[dst[j]] = k;
 			}
 		}
 		for(int i = tid; i < L::NW * kDigitBins; i += NT) sWarpHist[i] = 0;
 		__syncthreads();
 
-		// The key buffer and buffer 1 are free: the next tile's keys and this
-		// tile's second value array head there.
-		if(tid == 0) {
+		// The key buffer is free: the next tile's keys head there.
+		if(tid == 0 && nextBulk) {
 			fence_proxy_async_smem();
-			if(nextBulk) stage_tile(sKeys, a.buf.keysIn + next, kTileBytes, &sBar[0]);
-			if(bulk) stage_tile(sBuf1, a.buf.valsIn[1] + tileStart, kTileBytes, &sBar[2]);
+			stage_tile(sKeys, a.buf.keysIn + next, kTileBytes, &sBar[0]);
 		}
 
 #pragma unroll
 		for(int v = 0; v < NV; ++v) {
-			unsigned* buf = (v & 1) ? sBuf1 : sBuf0;
 			if(bulk) {
-				wait_bar((v & 1) ? 2 : 3);
+				wait_bar(1 + v);
+				const unsigned* buf = sm.staged(v);
 #pragma unroll
 				for(int j = 0; j < IPT; ++j)
 					if(dst[j] >= 0) a.buf.valsOut[v][dst[j]] = buf[src[j]];
@@ -924,22 +933,13 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 				for(int j = 0; j < IPT; ++j)
 					if(dst[j] >= 0) a.buf.valsOut[v][dst[j]] = in[src[j]];
 			}
-			if(v + 2 < NV) {
-				// Everyone has read the buffer: array v + 2 goes into it.
-				__syncthreads();
-				if(bulk && tid == 0) {
-					fence_proxy_async_smem();
-					stage_tile(buf, a.buf.valsIn[v + 2] + tileStart, kTileBytes,
-						&sBar[(v & 1) ? 2 : 3]);
-				}
-			}
 		}
 		__syncthreads();
 
-		// Buffer 0 is free: the next tile's first value array.
+		// Every staging buffer is free: the next tile's value arrays.
 		if(tid == 0 && nextBulk) {
 			fence_proxy_async_smem();
-			stage_tile(sBuf0, a.buf.valsIn[0] + next, kTileBytes, &sBar[3]);
+			stage_values(next);
 		}
 		tileStart = next;
 	}
