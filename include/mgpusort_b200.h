@@ -50,6 +50,20 @@ sortStatus_t SORTAPI sortEnableKernelTiming(sortEngine_t engine, int enable);
 sortStatus_t SORTAPI sortReadKernelTiming(sortEngine_t engine,
 	double* upsweepMs, int* upsweepLaunches, double* passMs, int* passLaunches);
 
+/* CUDA graphs of repeated sorts. When a call's launch sequence is the same
+ * as an earlier call's (same sizes, bit range, value mode, buffers and
+ * parity, same segment-offset pointer and count for sortSegmentedArray), the
+ * engine captures the sequence once as a CUDA graph and from then on
+ * replays it with one graph launch; buffer contents and segment boundaries
+ * may differ between calls. Calls with earlyExit, with kernel timing on or
+ * with an injected fault always launch directly. On by default; enable = 0
+ * turns it off and frees the cached graphs (at most 8 per engine). */
+sortStatus_t SORTAPI sortEnableGraphs(sortEngine_t engine, int enable);
+
+/* Graph replays since the engine was created, and graphs cached now. Either
+ * pointer may be NULL. */
+sortStatus_t SORTAPI sortGraphStats(sortEngine_t engine, int* replays, int* cached);
+
 /* Key types of sortArrayTyped. */
 typedef enum {
 	SORT_KEY_UINT32 = 0,

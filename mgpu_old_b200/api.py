@@ -77,7 +77,8 @@ EXPORTED_SYMBOLS = (
     # mgpusort_b200.h (no reference counterpart)
     "sortArrayAsync", "sortSynchronize", "sortPlanPasses", "sortInjectFault",
     "sortEnableKernelTiming", "sortReadKernelTiming", "sortArrayNoAlloc",
-    "sortSegmentedArray", "sortArrayTyped", "sortSelectKey", "sortServerCreate", "sortServerSubmit", "sortServerPoll",
+    "sortSegmentedArray", "sortArrayTyped", "sortSelectKey", "sortEnableGraphs",
+    "sortGraphStats", "sortServerCreate", "sortServerSubmit", "sortServerPoll",
     "sortServerWait", "sortServerDestroy",
     # mgpubwt.h (inc/mgpubwt.h, bwt/src/mgpubwt/bwt.def)
     "bwtStatusString", "bwtCreateEngine", "bwtDestroyEngine", "bwtSortBlock",
@@ -128,6 +129,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "sortSegmentedArray": (c_int, [engine_t, data_t, c_void_p, c_int, c_void_p]),
         "sortArrayTyped": (c_int, [engine_t, data_t, c_int, c_void_p]),
         "sortSelectKey": (c_int, [engine_t, data_t, c_int, POINTER(c_uint)]),
+        "sortEnableGraphs": (c_int, [engine_t, c_int]),
+        "sortGraphStats": (c_int, [engine_t, POINTER(c_int), POINTER(c_int)]),
         "sortServerCreate": (c_int, [POINTER(ServerConfig), POINTER(c_void_p)]),
         "sortServerSubmit": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                      c_void_p, c_void_p, POINTER(ctypes.c_ulonglong)]),
@@ -224,6 +227,15 @@ class MgpuSort:
         st = load_library().sortSelectKey(self._engine, ctypes.byref(data), int(k),
                                           ctypes.byref(v))
         return st, int(v.value)
+
+    def enable_graphs(self, enable: bool) -> int:
+        return load_library().sortEnableGraphs(self._engine, 1 if enable else 0)
+
+    def graph_stats(self) -> tuple[int, int]:
+        """(graph replays so far, graphs cached now)."""
+        r, c = c_int(0), c_int(0)
+        check(load_library().sortGraphStats(self._engine, ctypes.byref(r), ctypes.byref(c)))
+        return r.value, c.value
 
     def synchronize(self) -> int:
         return load_library().sortSynchronize(self._engine)

@@ -68,6 +68,33 @@ int round_up(int x, int m) { return (int)(((long long)x + m - 1) / m * m); }
 
 } // namespace
 
+// Everything the kernel arguments of one sort call depend on. Two calls with
+// equal keys launch the same kernels with the same arguments (the engine's
+// scratch is fixed while a key is cached), so a launch sequence captured as
+// a CUDA graph can be replayed for the second and later ones.
+struct GraphKey {
+	int kind;                   // 0: one array, 1: segmented
+	int bitPass;
+	int keyType;
+	int numElements;
+	int valueCount;
+	int firstBit;
+	int endBit;
+	int numSegments;
+	const int* offsets;
+	CUdeviceptr keys[2];
+	CUdeviceptr values[6][2];
+};
+
+struct CachedGraph {
+	GraphKey key;
+	cudaGraphExec_t exec;
+	int swaps;                  // buffer swaps the sequence makes
+	unsigned long long used;
+};
+
+constexpr size_t kGraphCacheSize = 8;
+
 struct sortEngine_d {
 	long refs = 1;
 	int device = 0;
@@ -91,6 +118,13 @@ struct sortEngine_d {
 	bool timing = false;
 	std::vector<TimedLaunch> timed;
 	size_t timedUsed = 0;
+	// CUDA graphs of launch sequences that repeat (sortEnableGraphs).
+	bool graphs = true;
+	cudaStream_t captureStream = nullptr;
+	std::vector<CachedGraph> graphCache;
+	std::vector<GraphKey> seenOnce;
+	unsigned long long graphClock = 0;
+	int graphReplays = 0;
 };
 
 namespace {
@@ -127,6 +161,8 @@ void destroy_engine(sortEngine_d* e) {
 		cudaEventDestroy(t.start);
 		cudaEventDestroy(t.stop);
 	}
+	for(auto& g : e->graphCache) cudaGraphExecDestroy(g.exec);
+	if(e->captureStream) cudaStreamDestroy(e->captureStream);
 	if(e->ctrl) cudaFree(e->ctrl);
 	if(e->scratch) cudaFree(e->scratch);
 	if(e->segScratch) cudaFree(e->segScratch);
@@ -198,6 +234,106 @@ void swap_buffers(sortData_d* d) {
 	d->parity ^= 1;
 }
 
+GraphKey graph_key(int kind, const sortData_d* d, int bitPass, int keyType,
+	const int* offsets, int numSegments) {
+	GraphKey k;
+	std::memset(&k, 0, sizeof(k));
+	k.kind = kind;
+	k.bitPass = bitPass;
+	k.keyType = keyType;
+	k.numElements = d->numElements;
+	k.valueCount = d->valueCount;
+	k.firstBit = d->firstBit;
+	k.endBit = d->endBit;
+	k.numSegments = numSegments;
+	k.offsets = offsets;
+	const int arrays = d->valueCount == -1 ? 1 : d->valueCount;
+	for(int j = 0; j < 2; ++j) {
+		k.keys[j] = d->keys[j];
+		for(int i = 0; i < arrays; ++i) k.values[i][j] = d->values[i][j];
+	}
+	return k;
+}
+
+bool same_key(const GraphKey& a, const GraphKey& b) {
+	return std::memcmp(&a, &b, sizeof(GraphKey)) == 0;
+}
+
+void drop_graphs(sortEngine_d* e) {
+	for(auto& g : e->graphCache) cudaGraphExecDestroy(g.exec);
+	e->graphCache.clear();
+	e->seenOnce.clear();
+}
+
+// Runs a launch sequence seq(d, stream, &swaps) on `stream`. A sequence whose
+// key was launched before is captured once into a CUDA graph on the
+// engine's capture stream and replayed from then on (one graph launch
+// instead of one launch per kernel); a key seen for the first time runs
+// directly, so one-off calls pay no capture. On replay the host side makes
+// the buffer swaps the sequence made when it was captured. If capture or
+// instantiation fails the sequence runs directly.
+template<typename Seq>
+sortStatus_t run_sequence(sortEngine_d* e, sortData_d* d, const GraphKey& key,
+	bool graphOk, cudaStream_t stream, Seq seq) {
+	int swaps = 0;
+	if(!graphOk || !e->graphs) return seq(d, stream, &swaps);
+	++e->graphClock;
+	for(auto& g : e->graphCache) {
+		if(!same_key(g.key, key)) continue;
+		if(cudaGraphLaunch(g.exec, stream) != cudaSuccess) {
+			cudaGetLastError();
+			return SORT_STATUS_LAUNCH_ERROR;
+		}
+		for(int i = 0; i < g.swaps; ++i) swap_buffers(d);
+		g.used = e->graphClock;
+		++e->graphReplays;
+		return SORT_STATUS_SUCCESS;
+	}
+	bool seen = false;
+	for(auto& k : e->seenOnce) seen = seen || same_key(k, key);
+	if(!seen) {
+		if(e->seenOnce.size() >= kGraphCacheSize) e->seenOnce.erase(e->seenOnce.begin());
+		e->seenOnce.push_back(key);
+		return seq(d, stream, &swaps);
+	}
+
+	// Second sighting: capture. The capture stream first waits for the
+	// caller's stream (no work is captured from it; the graph launch below
+	// is what orders after it).
+	sortData_d shadow = *d;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	sortStatus_t st = SORT_STATUS_INTERNAL_ERROR;
+	if(cudaStreamBeginCapture(e->captureStream, cudaStreamCaptureModeThreadLocal)
+		== cudaSuccess) {
+		st = seq(&shadow, e->captureStream, &swaps);
+		const cudaError_t ce = cudaStreamEndCapture(e->captureStream, &graph);
+		if(ce != cudaSuccess) st = SORT_STATUS_INTERNAL_ERROR;
+	}
+	if(st == SORT_STATUS_SUCCESS && graph &&
+		cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+		exec = nullptr;
+	if(graph) cudaGraphDestroy(graph);
+	if(st != SORT_STATUS_SUCCESS || !exec) {
+		cudaGetLastError();
+		if(exec) cudaGraphExecDestroy(exec);
+		return seq(d, stream, &swaps);
+	}
+	if(e->graphCache.size() >= kGraphCacheSize) {
+		auto lru = std::min_element(e->graphCache.begin(), e->graphCache.end(),
+			[](const CachedGraph& a, const CachedGraph& b) { return a.used < b.used; });
+		cudaGraphExecDestroy(lru->exec);
+		e->graphCache.erase(lru);
+	}
+	e->graphCache.push_back(CachedGraph{key, exec, swaps, e->graphClock});
+	if(cudaGraphLaunch(exec, stream) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_LAUNCH_ERROR;
+	}
+	for(int i = 0; i < swaps; ++i) swap_buffers(d);
+	return SORT_STATUS_SUCCESS;
+}
+
 // The whole sort of one sortData_d: validation, upsweep, the pass loop.
 // bitPass 0 selects sortArray's plan, 1..6 sortArrayEx's. Signed and float
 // keys (keyType) are mapped to their uint32 image in place before the first
@@ -234,73 +370,84 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 		e->dirty = false;
 	}
 
-	cudaError_t ce = mgpusort::launch_key_transform(
-		reinterpret_cast<unsigned*>(d->keys[0]), n, keyType, true, stream);
-	if(ce != cudaSuccess) return launch_status(ce);
-
 	bool bulk = true;
 	for(int i = 0; i < 2; ++i) bulk = bulk && aligned16(d->keys[i]);
 	for(int i = 0; i < numArrays; ++i)
 		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
 
-	// earlyExit: one upsweep builds every pass's digit histogram, one
-	// read-back of the per-pass "single digit" flags, then those passes are
-	// skipped (the reference reads its detect counters back per pass for the
-	// same purpose, mgpusort.cpp:434-451). Without earlyExit a single-digit
-	// pass runs as a straight copy.
-	bool skip[mgpusort::kMaxPasses] = {};
-	int slot = -1;
-	if(d->earlyExit) {
-		slot = timing_begin(e, kTimedUpsweep, stream);
-		ce = mgpusort::launch_upsweep(
-			reinterpret_cast<const unsigned*>(d->keys[0]), n, plan, e->ctrl,
-			e->hostErrorDev, e->numSMs, stream);
-		timing_end(e, slot, stream);
-		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-		if(cudaMemcpyAsync(e->hostTrivial, e->ctrl->trivial,
-			sizeof(unsigned) * plan.numPasses, cudaMemcpyDeviceToHost, stream)
-			!= cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
-			e->dirty = true;
-			return SORT_STATUS_DEVICE_ERROR;
-		}
-		for(int p = 0; p < plan.numPasses; ++p) skip[p] = e->hostTrivial[p] != 0;
-	}
-
-	bool firstExecuted = true;
-	for(int p = 0; p < plan.numPasses; ++p) {
-		if(skip[p]) continue;
-		const int vm = (indexMode && firstExecuted) ? mgpusort::kValueIndex
-			: numArrays;
-		mgpusort::PassBuffers buf = {};
-		buf.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
-		buf.keysOut = reinterpret_cast<unsigned*>(d->keys[1]);
-		for(int i = 0; i < 6; ++i) {
-			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
-			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
-		}
-		slot = timing_begin(e, kTimedUpsweep, stream);
-		ce = mgpusort::launch_pass_count(buf, vm, n, p, plan, e->scratch, e->numSMs,
-			stream);
-		timing_end(e, slot, stream);
-		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-		slot = timing_begin(e, kTimedPass, stream);
-		ce = mgpusort::launch_pass_sort(buf, vm, n, p, plan, e->ctrl, e->scratch,
-			bulk, e->failTile, e->hostErrorDev, e->numSMs, stream);
-		timing_end(e, slot, stream);
-		e->failTile = -1;
-		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-		swap_buffers(d);
-		firstExecuted = false;
-	}
-	if(indexMode && firstExecuted) {
-		// Every pass was skipped: the identity order still needs its indices.
-		ce = mgpusort::launch_iota(reinterpret_cast<unsigned*>(d->values1[0]), n,
-			stream);
+	auto seq = [&](sortData_d* sd, cudaStream_t st, int* swaps) -> sortStatus_t {
+		cudaError_t ce = mgpusort::launch_key_transform(
+			reinterpret_cast<unsigned*>(sd->keys[0]), n, keyType, true, st);
 		if(ce != cudaSuccess) return launch_status(ce);
-	}
-	ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(d->keys[0]), n,
-		keyType, false, stream);
-	if(ce != cudaSuccess) return launch_status(ce);
+
+		// earlyExit: one upsweep builds every pass's digit histogram, one
+		// read-back of the per-pass "single digit" flags, then those passes
+		// are skipped (the reference reads its detect counters back per pass
+		// for the same purpose, mgpusort.cpp:434-451). Without earlyExit a
+		// single-digit pass runs as a straight copy.
+		bool skip[mgpusort::kMaxPasses] = {};
+		int slot = -1;
+		if(sd->earlyExit) {
+			slot = timing_begin(e, kTimedUpsweep, st);
+			ce = mgpusort::launch_upsweep(
+				reinterpret_cast<const unsigned*>(sd->keys[0]), n, plan, e->ctrl,
+				e->hostErrorDev, e->numSMs, st);
+			timing_end(e, slot, st);
+			if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+			if(cudaMemcpyAsync(e->hostTrivial, e->ctrl->trivial,
+				sizeof(unsigned) * plan.numPasses, cudaMemcpyDeviceToHost, st)
+				!= cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+				e->dirty = true;
+				return SORT_STATUS_DEVICE_ERROR;
+			}
+			for(int p = 0; p < plan.numPasses; ++p) skip[p] = e->hostTrivial[p] != 0;
+		}
+
+		bool firstExecuted = true;
+		for(int p = 0; p < plan.numPasses; ++p) {
+			if(skip[p]) continue;
+			const int vm = (indexMode && firstExecuted) ? mgpusort::kValueIndex
+				: numArrays;
+			mgpusort::PassBuffers buf = {};
+			buf.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+			buf.keysOut = reinterpret_cast<unsigned*>(sd->keys[1]);
+			for(int i = 0; i < 6; ++i) {
+				buf.valsIn[i] = reinterpret_cast<const unsigned*>(sd->values[i][0]);
+				buf.valsOut[i] = reinterpret_cast<unsigned*>(sd->values[i][1]);
+			}
+			slot = timing_begin(e, kTimedUpsweep, st);
+			ce = mgpusort::launch_pass_count(buf, vm, n, p, plan, e->scratch,
+				e->numSMs, st);
+			timing_end(e, slot, st);
+			if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+			slot = timing_begin(e, kTimedPass, st);
+			ce = mgpusort::launch_pass_sort(buf, vm, n, p, plan, e->ctrl, e->scratch,
+				bulk, e->failTile, e->hostErrorDev, e->numSMs, st);
+			timing_end(e, slot, st);
+			e->failTile = -1;
+			if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+			swap_buffers(sd);
+			++*swaps;
+			firstExecuted = false;
+		}
+		if(indexMode && firstExecuted) {
+			// Every pass was skipped: the identity order still needs its
+			// indices.
+			ce = mgpusort::launch_iota(reinterpret_cast<unsigned*>(sd->values1[0]), n,
+				st);
+			if(ce != cudaSuccess) return launch_status(ce);
+		}
+		ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(sd->keys[0]), n,
+			keyType, false, st);
+		return launch_status(ce);
+	};
+
+	// earlyExit decides on the host mid-sequence; timing and fault
+	// injection are per call: those run directly.
+	const bool graphOk = !d->earlyExit && !e->timing && e->failTile < 0;
+	const sortStatus_t rs = run_sequence(e, d,
+		graph_key(0, d, bitPass, keyType, nullptr, 0), graphOk, stream, seq);
+	if(rs != SORT_STATUS_SUCCESS) return rs;
 	cudaEventRecord(e->done, stream);
 	return SORT_STATUS_SUCCESS;
 }
@@ -342,6 +489,7 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 
 	const size_t bytes = mgpusort::seg_scratch_bytes(n, numSegments);
 	if(bytes > e->segScratchBytes) {
+		drop_graphs(e);
 		if(e->segScratch) cudaFree(e->segScratch);
 		e->segScratch = nullptr;
 		e->segScratchBytes = 0;
@@ -363,42 +511,50 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
 
 	const int firstMode = indexMode ? mgpusort::kValueIndex : numArrays;
-	cudaError_t ce = mgpusort::launch_seg_plan(offsets, numSegments, n, firstMode,
-		e->segScratch, e->ctrl, e->hostErrorDev, stream);
-	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-
-	// Segments of up to 4096 elements: every pass in shared memory, straight
-	// into the buffers that hold the result after all passes' swaps.
-	const int last = plan.numPasses & 1;
-	mgpusort::PassBuffers small = {};
-	small.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
-	small.keysOut = reinterpret_cast<unsigned*>(d->keys[last]);
-	for(int i = 0; i < 6; ++i) {
-		small.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
-		small.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][last]);
-	}
-	int slot = timing_begin(e, kTimedUpsweep, stream);
-	ce = mgpusort::launch_seg_small(small, firstMode, plan, offsets, numSegments, n,
-		e->segScratch, e->numSMs, stream);
-	timing_end(e, slot, stream);
-	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-
-	for(int p = 0; p < plan.numPasses; ++p) {
-		const int vm = (indexMode && p == 0) ? mgpusort::kValueIndex : numArrays;
-		mgpusort::PassBuffers buf = {};
-		buf.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
-		buf.keysOut = reinterpret_cast<unsigned*>(d->keys[1]);
-		for(int i = 0; i < 6; ++i) {
-			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
-			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
-		}
-		slot = timing_begin(e, kTimedPass, stream);
-		ce = mgpusort::launch_seg_pass(buf, vm, p, plan, offsets, numSegments, n,
-			e->segScratch, e->ctrl, bulk, e->hostErrorDev, e->numSMs, stream);
-		timing_end(e, slot, stream);
+	auto seq = [&](sortData_d* sd, cudaStream_t st, int* swaps) -> sortStatus_t {
+		cudaError_t ce = mgpusort::launch_seg_plan(offsets, numSegments, n, firstMode,
+			e->segScratch, e->ctrl, e->hostErrorDev, st);
 		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
-		swap_buffers(d);
-	}
+
+		// Segments of up to 4096 elements: every pass in shared memory,
+		// straight into the buffers that hold the result after all passes'
+		// swaps.
+		const int last = plan.numPasses & 1;
+		mgpusort::PassBuffers small = {};
+		small.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+		small.keysOut = reinterpret_cast<unsigned*>(sd->keys[last]);
+		for(int i = 0; i < 6; ++i) {
+			small.valsIn[i] = reinterpret_cast<const unsigned*>(sd->values[i][0]);
+			small.valsOut[i] = reinterpret_cast<unsigned*>(sd->values[i][last]);
+		}
+		int slot = timing_begin(e, kTimedUpsweep, st);
+		ce = mgpusort::launch_seg_small(small, firstMode, plan, offsets, numSegments, n,
+			e->segScratch, e->numSMs, st);
+		timing_end(e, slot, st);
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+
+		for(int p = 0; p < plan.numPasses; ++p) {
+			const int vm = (indexMode && p == 0) ? mgpusort::kValueIndex : numArrays;
+			mgpusort::PassBuffers buf = {};
+			buf.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+			buf.keysOut = reinterpret_cast<unsigned*>(sd->keys[1]);
+			for(int i = 0; i < 6; ++i) {
+				buf.valsIn[i] = reinterpret_cast<const unsigned*>(sd->values[i][0]);
+				buf.valsOut[i] = reinterpret_cast<unsigned*>(sd->values[i][1]);
+			}
+			slot = timing_begin(e, kTimedPass, st);
+			ce = mgpusort::launch_seg_pass(buf, vm, p, plan, offsets, numSegments, n,
+				e->segScratch, e->ctrl, bulk, e->hostErrorDev, e->numSMs, st);
+			timing_end(e, slot, st);
+			if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+			swap_buffers(sd);
+			++*swaps;
+		}
+		return SORT_STATUS_SUCCESS;
+	};
+	const sortStatus_t rs = run_sequence(e, d,
+		graph_key(1, d, 0, 0, offsets, numSegments), !e->timing, stream, seq);
+	if(rs != SORT_STATUS_SUCCESS) return rs;
 	cudaEventRecord(e->done, stream);
 	return SORT_STATUS_SUCCESS;
 }
@@ -469,7 +625,8 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 		e->hostTrivial = static_cast<unsigned*>(h);
 	}
 	if(status == SORT_STATUS_SUCCESS &&
-		cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess)
+		(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess ||
+		cudaStreamCreateWithFlags(&e->captureStream, cudaStreamNonBlocking) != cudaSuccess))
 		status = SORT_STATUS_DEVICE_ERROR;
 	if(status != SORT_STATUS_SUCCESS) {
 		cudaGetLastError();
@@ -638,6 +795,20 @@ int SORTAPI sortPlanPasses(int firstBit, int endBit, int bitPass,
 	if(bitPass < 0 || bitPass > 6) return -1;
 	return bitPass ? plan_widths_reference(numBits, bitPass, widths)
 		: plan_widths_default(numBits, widths);
+}
+
+sortStatus_t SORTAPI sortEnableGraphs(sortEngine_t engine, int enable) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	engine->graphs = enable != 0;
+	if(!engine->graphs) drop_graphs(engine);
+	return SORT_STATUS_SUCCESS;
+}
+
+sortStatus_t SORTAPI sortGraphStats(sortEngine_t engine, int* replays, int* cached) {
+	if(!engine) return SORT_STATUS_INVALID_VALUE;
+	if(replays) *replays = engine->graphReplays;
+	if(cached) *cached = (int)engine->graphCache.size();
+	return SORT_STATUS_SUCCESS;
 }
 
 sortStatus_t SORTAPI sortInjectFault(sortEngine_t engine, int tile) {

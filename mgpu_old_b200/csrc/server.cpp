@@ -298,6 +298,10 @@ sortStatus_t SORTAPI sortServerCreate(const sortServerConfig* config,
 			sortServerDestroy(s.release());
 			return st;
 		}
+		// Batches come from a memory pool at varying addresses and sizes:
+		// their launch sequences seldom repeat, so slots launch directly
+		// rather than capture graphs.
+		sortEnableGraphs(slot.engine, 0);
 		void* h = nullptr;
 		if(cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) != cudaSuccess ||
