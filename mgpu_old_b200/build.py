@@ -55,28 +55,40 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(f) <= t for f in _inputs())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every source into the shared library; return its path."""
-    if not force and up_to_date():
-        return LIB_PATH
-    objdir = os.path.join(HERE, "_build")
+def _compile(lib_path: str, objdir: str, defines: dict | None, verbose: bool) -> str:
     os.makedirs(objdir, exist_ok=True)
+    extra = [f"-D{k}={v}" for k, v in (defines or {}).items()]
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-c", os.path.join(CSRC, src),
+               "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    tmp = LIB_PATH + ".tmp"
+    tmp = lib_path + ".tmp"
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
            "-Xcompiler", "-fPIC", *objs, "-o", tmp]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, lib_path)
+    return lib_path
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source into the shared library; return its path."""
+    if not force and up_to_date():
+        return LIB_PATH
+    return _compile(LIB_PATH, os.path.join(HERE, "_build"), None, verbose)
+
+
+def build_variant(name: str, defines: dict, verbose: bool = False) -> str:
+    """The library with tile_config.h values overridden by `defines`, built
+    under _build/tune/<name>/ (for the autotuner); returns its path."""
+    d = os.path.join(HERE, "_build", "tune", name)
+    return _compile(os.path.join(d, LIB_NAME), d, defines, verbose)
 
 
 if __name__ == "__main__":

@@ -15,6 +15,7 @@
 #include "../../include/mgpusort_b200.h"
 #pragma GCC visibility pop
 #include "sort_kernels.h"
+#include "tile_config.h"
 
 #include <cuda_runtime.h>
 
@@ -172,10 +173,13 @@ void destroy_engine(sortEngine_d* e) {
 	delete e;
 }
 
-// sortArray's plan: the fewest passes of at most 8 bits, widths balanced
-// (wider passes first), least significant digit first.
+// sortArray's plan: the fewest passes of at most MGPU_SORT_MAX_DIGIT_BITS
+// (8) bits, widths balanced (wider passes first), least significant digit
+// first.
 int plan_widths_default(int numBits, int* widths) {
-	int passes = (numBits + 7) / 8;
+	constexpr int kWidth = MGPU_SORT_MAX_DIGIT_BITS;
+	static_assert(kWidth >= 1 && kWidth <= 8, "digits of 1..8 bits");
+	int passes = (numBits + kWidth - 1) / kWidth;
 	for(int p = 0; p < passes; ++p)
 		widths[p] = numBits / passes + (p < numBits % passes ? 1 : 0);
 	return passes;

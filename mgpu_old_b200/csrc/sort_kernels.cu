@@ -23,6 +23,7 @@
 
 #include "sort_kernels.h"
 #include "sort_device.cuh"
+#include "tile_config.h"
 
 #include <algorithm>
 
@@ -367,24 +368,27 @@ struct SortArgs {
 	int failTile;                   // tile whose CTA runs a wait out; -1: none
 };
 
-// Tile shapes measured on B200 (sort kernel time over 32 Mi and 64 Mi
-// key-value pairs, 256..512 threads x 12..32 keys): larger tiles give each
-// digit longer runs per tile, so fewer partially written sectors reach DRAM;
-// 384 x 20 was best for keys, indices and one value array (256 x 20 with
-// three CTAs per SM was 2% faster at 32 Mi skewed keys but 29% slower at
-// 64 Mi uniform keys: more ranges, more write fronts). Several value arrays
-// multiply the write fronts (ranges x digits x arrays), and a front is
-// revisited only once per tile of its range, so partial sectors leave L2
-// before they are completed: one CTA of 768 x 8 per SM halves the ranges and
-// was 1.21x faster than two of 384 x 16 at 16 Mi keys with six arrays.
 // mbarriers of a sort CTA: keys, up to six value arrays, the fault wait.
 constexpr int kNumBars = 8;
 constexpr int kFaultBar = 7;
 
+// Tile shapes (tile_config.h, chosen by the autotuner). What the
+// measurements showed: larger tiles give each digit longer runs per tile,
+// so fewer partially written sectors reach DRAM; for keys, indices and one
+// value array two CTAs of 384 x 20 per SM were best (256 x 20 with three
+// CTAs per SM was 2% faster at 32 Mi skewed keys but 29% slower at 64 Mi
+// uniform keys: more ranges, more write fronts; one CTA per SM lost the
+// overlap of one CTA's ranking with the other's stores). Several value
+// arrays multiply the write fronts (ranges x digits x arrays), and a front
+// is revisited only once per tile of its range, so partial sectors leave L2
+// before they are completed: one CTA of 768 x 8 per SM halves the ranges.
 template<int VM> struct SortConfig {
-	static constexpr int kThreads = VM >= 2 ? 768 : 384;
-	static constexpr int kItems = VM >= 2 ? 8 : 20;
-	static constexpr int kMinBlocks = VM >= 2 ? 1 : 2;
+	static constexpr int kThreads = VM >= 2 ? MGPU_SORT_MULTI_THREADS
+		: VM == 0 ? MGPU_SORT_KEYS_THREADS : MGPU_SORT_SINGLE_THREADS;
+	static constexpr int kItems = VM >= 2 ? MGPU_SORT_MULTI_ITEMS
+		: VM == 0 ? MGPU_SORT_KEYS_ITEMS : MGPU_SORT_SINGLE_ITEMS;
+	static constexpr int kMinBlocks = VM >= 2 ? MGPU_SORT_MULTI_MIN_BLOCKS
+		: VM == 0 ? MGPU_SORT_KEYS_MIN_BLOCKS : MGPU_SORT_SINGLE_MIN_BLOCKS;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;

@@ -1,0 +1,67 @@
+// Tile shapes and digit width of the sort passes.
+//
+// These values are the choices of the autotuner (mgpu_old_b200/autotune.py),
+// which builds the library once per candidate shape, times each build on a
+// B200 over a fixed set of workloads and writes this file with the fastest
+// shape per class. Every value can be overridden at build time with -D.
+//
+//  * keys: keys only (sort_range_single without values);
+//  * single: index mode or one value array (sort_range_single);
+//  * multi: two to six value arrays (sort_range_multi).
+// Measured by the autotuner (median ms per sort; score = geometric
+// mean of time / best time over the class's workloads):
+//   keys: chosen 256x20x3
+//       256x20x3  score 1.032  keys_u32_1048576 0.076, keys_u32_16777216 0.403, keys_u32_67108864 1.401
+//       512x14x2  score 1.043  keys_u32_1048576 0.080, keys_u32_16777216 0.385, keys_u32_67108864 1.438
+//       384x20x2  score 1.050  keys_u32_1048576 0.082, keys_u32_16777216 0.397, keys_u32_67108864 1.387
+//       512x16x2  score 1.053  keys_u32_1048576 0.084, keys_u32_16777216 0.381, keys_u32_67108864 1.423
+//       384x24x2  score 1.059  keys_u32_1048576 0.090, keys_u32_16777216 0.379, keys_u32_67108864 1.358
+//   single: chosen 384x20x2
+//       384x20x2  score 1.000  index_u32_16777216 0.496, pairs_and24_33554432 0.676, pairs_u32_67108864 1.729
+//       512x14x2  score 1.021  index_u32_16777216 0.500, pairs_and24_33554432 0.696, pairs_u32_67108864 1.772
+//       256x24x2  score 1.028  index_u32_16777216 0.498, pairs_and24_33554432 0.686, pairs_u32_67108864 1.839
+//       384x16x2  score 1.029  index_u32_16777216 0.500, pairs_and24_33554432 0.690, pairs_u32_67108864 1.827
+//       768x10x1  score 1.108  index_u32_16777216 0.526, pairs_and24_33554432 0.764, pairs_u32_67108864 1.957
+//       256x20x3  score 1.145  index_u32_16777216 0.571, pairs_and24_33554432 0.693, pairs_u32_67108864 2.193
+//   multi: chosen 768x8x1
+//        768x8x1  score 1.002  multi3_u32_16777216 0.879, multi6_17bit_16777216 1.217
+//       512x12x1  score 1.008  multi3_u32_16777216 0.874, multi6_17bit_16777216 1.235
+//       384x16x1  score 1.022  multi3_u32_16777216 0.881, multi6_17bit_16777216 1.262
+//       576x10x1  score 1.033  multi3_u32_16777216 0.899, multi6_17bit_16777216 1.264
+//   digits: chosen 8
+//              8  score 1.000  keys_u32_16777216 0.397, pairs_and24_33554432 0.674
+//              7  score 1.230  keys_u32_16777216 0.481, pairs_and24_33554432 0.842
+//              6  score 1.333  keys_u32_16777216 0.565, pairs_and24_33554432 0.842
+#pragma once
+
+#ifndef MGPU_SORT_KEYS_THREADS
+#define MGPU_SORT_KEYS_THREADS 256
+#endif
+#ifndef MGPU_SORT_KEYS_ITEMS
+#define MGPU_SORT_KEYS_ITEMS 20
+#endif
+#ifndef MGPU_SORT_KEYS_MIN_BLOCKS
+#define MGPU_SORT_KEYS_MIN_BLOCKS 3
+#endif
+#ifndef MGPU_SORT_SINGLE_THREADS
+#define MGPU_SORT_SINGLE_THREADS 384
+#endif
+#ifndef MGPU_SORT_SINGLE_ITEMS
+#define MGPU_SORT_SINGLE_ITEMS 20
+#endif
+#ifndef MGPU_SORT_SINGLE_MIN_BLOCKS
+#define MGPU_SORT_SINGLE_MIN_BLOCKS 2
+#endif
+#ifndef MGPU_SORT_MULTI_THREADS
+#define MGPU_SORT_MULTI_THREADS 768
+#endif
+#ifndef MGPU_SORT_MULTI_ITEMS
+#define MGPU_SORT_MULTI_ITEMS 8
+#endif
+#ifndef MGPU_SORT_MULTI_MIN_BLOCKS
+#define MGPU_SORT_MULTI_MIN_BLOCKS 1
+#endif
+// Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
+#ifndef MGPU_SORT_MAX_DIGIT_BITS
+#define MGPU_SORT_MAX_DIGIT_BITS 8
+#endif
