@@ -217,7 +217,12 @@ def cpu_sort_sample(case, sample_n, threads):
     p = (bits + 7) // 8
     widths = [bits // p + (i < bits % p) for i in range(p)]
     t0 = time.perf_counter()
+    if case.key_type:
+        # Signed / float keys: the same transform, sort and inverse on the host.
+        keys = workloads.key_image(keys, case.key_type)
     oracle.sort_lsd(keys, vals, case.value_count, case.first_bit, widths, 1 << 15, threads)
+    if case.key_type:
+        keys = workloads.key_preimage(keys, case.key_type)
     return time.perf_counter() - t0
 
 
@@ -496,7 +501,7 @@ def verify(case, keys, vals):
     workloads the exact stable permutation."""
     bits = case.end_bit - case.first_bit
     mask = np.uint32(0xFFFFFFFF if bits >= 32 else (1 << bits) - 1)
-    f = (keys >> np.uint32(case.first_bit)) & mask
+    f = (workloads.key_image(keys, case.key_type) >> np.uint32(case.first_bit)) & mask
     assert (f[1:] >= f[:-1]).all(), "output not ordered"
     assert np.array_equal(np.sort(keys), np.sort(case.keys)), "keys not a permutation"
     if case.value_count == 1 and np.array_equal(case.values[0][:16], np.arange(16)):
@@ -869,7 +874,10 @@ def main():
     stream = torch.cuda.current_stream(device)
 
     def one_sort():
-        api.check(engine.sort_array(d))
+        if case.key_type:
+            api.check(engine.sort_array_typed(d, case.key_type, stream.cuda_stream))
+        else:
+            api.check(engine.sort_array(d))
 
     # Warm-up.
     for _ in range(max(args.warmup, 3)):
@@ -962,7 +970,10 @@ def main():
             srt.bufs[dd.keys[0]][:case.n].copy_(pinned_in[0], non_blocking=True)
             for i in range(len(case.values)):
                 srt.bufs[dd.values[i][0]][:case.n].copy_(pinned_in[1 + i], non_blocking=True)
-            api.check(eng.sort_array_async(dd, st.cuda_stream))
+            if case.key_type:
+                api.check(eng.sort_array_typed(dd, case.key_type, st.cuda_stream))
+            else:
+                api.check(eng.sort_array_async(dd, st.cuda_stream))
             out[0].copy_(srt.bufs[dd.keys[0]][:case.n], non_blocking=True)
             for i in range(srt.arrays):
                 out[1 + i].copy_(srt.bufs[dd.values[i][0]][:case.n], non_blocking=True)

@@ -20,6 +20,7 @@ class SortCase:
     value_count: int = 0          # -1 index mode, 0 keys only, 1..6
     first_bit: int = 0
     end_bit: int = 32
+    key_type: int = 0             # 0 uint32, 1 int32, 2 float32 (sortArrayTyped)
 
     @property
     def n(self) -> int:
@@ -101,6 +102,39 @@ def segments_lognormal(num_segments: int = 10_000, seed: int = 4,
     return SegmentedCase(name, keys, [local], 1, 0, 32, offsets.astype(np.int32))
 
 
+def key_image(keys: np.ndarray, key_type: int) -> np.ndarray:
+    """The order-preserving uint32 image of int32 (1) or float32 (2) key
+    bit patterns (identity for uint32)."""
+    keys = np.asarray(keys, dtype=np.uint32)
+    if key_type == 1:
+        return keys ^ np.uint32(0x80000000)
+    if key_type == 2:
+        neg = (keys >> np.uint32(31)) == 1
+        return np.where(neg, ~keys, keys ^ np.uint32(0x80000000)).astype(np.uint32)
+    return keys
+
+
+def key_preimage(image: np.ndarray, key_type: int) -> np.ndarray:
+    """Inverse of key_image."""
+    image = np.asarray(image, dtype=np.uint32)
+    if key_type == 1:
+        return image ^ np.uint32(0x80000000)
+    if key_type == 2:
+        pos = (image >> np.uint32(31)) == 1
+        return np.where(pos, image ^ np.uint32(0x80000000), ~image).astype(np.uint32)
+    return image
+
+
+def pairs_float32(n: int = 1 << 25, seed: int = 10) -> SortCase:
+    """Key-value with float32 keys (sortArrayTyped): normal values scaled by
+    10^[-30, 30), value = index, full 32-bit image. 33,554,432 pairs."""
+    rng = np.random.default_rng(seed)
+    f = (rng.standard_normal(n) * 10.0 ** rng.integers(-30, 30, n)).astype(np.float32)
+    return SortCase("pairs_f32_32M" if n == 1 << 25 else f"pairs_f32_{n}",
+                    f.view(np.uint32).copy(), [np.arange(n, dtype=np.uint32)], 1, 0, 32,
+                    key_type=2)
+
+
 def keys_uniform32_64m() -> SortCase:
     """Keys-only, uniform over 32 bits, 64Mi keys (a large keys-only case)."""
     c = keys_uniform32(1 << 26, seed=6)
@@ -136,6 +170,7 @@ WORKLOADS = {
     "multi6_17bit_16M": multi6_17bit,
     "pairs_u32_64M": pairs_uniform32,
     "keys_u32_64M": keys_uniform32_64m,
+    "pairs_f32_32M": pairs_float32,
     "segments_10k": segments_lognormal,
     "segments_10k_64M": lambda: segments_lognormal(scale_to=1 << 26),
 }

@@ -149,3 +149,18 @@ def test_oracle_bwt_matches_reference_quicksort(oracle_mod, kind, n):
     sym = np.concatenate([blk, blk])
     for i in np.nonzero(idx != ref_idx)[0]:
         assert bytes(sym[idx[i]:idx[i] + n]) == bytes(sym[ref_idx[i]:ref_idx[i] + n])
+
+
+def test_key_image_round_trip_and_order():
+    """The host restatement of the int32/float32 key image (used by the
+    bench's checks): a bijection that orders numerically."""
+    from mgpu_old_b200 import workloads as w
+    rng = np.random.default_rng(1)
+    k = rng.integers(0, 2 ** 32, 100_000, dtype=np.uint64).astype(np.uint32)
+    for t in (0, 1, 2):
+        assert np.array_equal(w.key_preimage(w.key_image(k, t), t), k)
+    f = np.array([-np.inf, -1.5, -1e-40, -0.0, 0.0, 1e-40, 2.0, np.inf],
+                 dtype=np.float32).view(np.uint32)
+    assert (np.diff(w.key_image(f, 2).astype(np.int64)) > 0).all()
+    i = np.array([-2 ** 31, -1, 0, 1, 2 ** 31 - 1], dtype=np.int32).view(np.uint32)
+    assert (np.diff(w.key_image(i, 1).astype(np.int64)) > 0).all()
