@@ -99,7 +99,7 @@ def segments_lognormal(num_segments: int = 10_000, seed: int = 4,
     keys = _u32(_rng(seed + 100), n)
     local = (np.arange(n, dtype=np.int64) - np.repeat(offsets[:-1], sizes)).astype(np.uint32)
     name = f"segments_{num_segments}_lognormal" + (f"_scaled{scale_to}" if scale_to else "")
-    return SegmentedCase(name, keys, [local], 1, 0, 32, offsets.astype(np.int32))
+    return SegmentedCase(name, keys, [local], 1, 0, 32, offsets=offsets.astype(np.int32))
 
 
 def key_image(keys: np.ndarray, key_type: int) -> np.ndarray:

@@ -164,3 +164,15 @@ def test_key_image_round_trip_and_order():
     assert (np.diff(w.key_image(f, 2).astype(np.int64)) > 0).all()
     i = np.array([-2 ** 31, -1, 0, 1, 2 ** 31 - 1], dtype=np.int32).view(np.uint32)
     assert (np.diff(w.key_image(i, 1).astype(np.int64)) > 0).all()
+
+
+def test_workload_generators_fields():
+    """Workload dataclasses keep their fields in place (segment offsets,
+    key types) at small sizes."""
+    from mgpu_old_b200 import workloads as w
+    seg = w.segments_lognormal(50)
+    assert seg.offsets is not None and seg.offsets.size == 51 and seg.key_type == 0
+    assert int(seg.offsets[-1]) == seg.n
+    f = w.pairs_float32(1000)
+    assert f.key_type == 2 and f.value_count == 1
+    assert w.pairs_and24(1000).key_type == 0
