@@ -1007,6 +1007,15 @@ sort_kernel(const SortArgs a) {
 // over device-side work lists, so the launch shapes do not depend on the
 // segment sizes.
 
+// Segmented-plan counters (ints): [0] tiny segments, [1] small, [2] large,
+// [3] ranges; from kSegWork, work counters the persistent kernels draw their
+// next item from: per pass p, [kSegWork + 2p] (count) and [kSegWork + 2p + 1]
+// (sort); then the tiny and small lists' (kSegWorkSmall, + 1). The plan
+// kernel zeroes them at the start of every sort.
+constexpr int kSegWork = 8;
+constexpr int kSegWorkSmall = kSegWork + 2 * kMaxPasses;
+constexpr int kSegCounters = kSegWorkSmall + 2;
+
 constexpr int kSegTinyMax = 512;
 constexpr int kSegSmallMax = 4096;
 constexpr int kSegMaxRangesPerSegment = 64;
@@ -1088,6 +1097,7 @@ __global__ void __launch_bounds__(kPlanThreads) seg_plan_kernel(const SegPlanArg
 		}
 		return;
 	}
+	for(int i = kSegWork + tid; i < kSegCounters; i += kPlanThreads) a.counters[i] = 0;
 
 	int nt = 0, ns = 0, nl = 0, nr = 0;
 	for(int s = s0; s < s1; ++s) {
@@ -1145,7 +1155,8 @@ struct SegCountArgs {
 	const unsigned* keys;
 	const int* rangeBegin;
 	const int* rangeEnd;
-	const int* counters;
+	int* counters;
+	int work;                       // counters[work]: next range to count
 	int shift;
 	int width;
 	int vecOk;
@@ -1158,13 +1169,18 @@ __global__ void __launch_bounds__(kCountThreads) seg_count_kernel(const SegCount
 	const int lane = tid & 31;
 	const unsigned mask = (1u << a.width) - 1;
 	const int shift = a.shift;
+	__shared__ int sNext;
 	const int R = a.counters[3];
 	unsigned* myCol = sHist + lane;
 	auto add = [&](unsigned k) { atomicAdd(&myCol[((k >> shift) & mask) * 32], 1u); };
 
-	for(int r = blockIdx.x; r < R; r += gridDim.x) {
+	// Ranges differ in size: each CTA draws the next one when done.
+	for(;;) {
+		if(tid == 0) sNext = atomicAdd(&a.counters[a.work], 1);
 		for(int i = tid; i < kDigitBins * 32; i += kCountThreads) sHist[i] = 0;
 		__syncthreads();
+		const int r = sNext;
+		if(r >= R) break;
 		const int begin = a.rangeBegin[r];
 		const int end = a.rangeEnd[r];
 		int e = begin;
@@ -1248,7 +1264,8 @@ struct SegSortArgs {
 	const int* rangeBegin;
 	const int* rangeEnd;
 	const int* rangeSeg;
-	const int* counters;
+	int* counters;
+	int work;                       // counters[work]: next range to sort
 	const unsigned* rangeStart;
 	const unsigned* rangeTrivial;
 };
@@ -1259,10 +1276,16 @@ seg_sort_kernel(const SegSortArgs a) {
 	extern __shared__ __align__(128) unsigned smem[];
 	const SortSmem<VM> sm(smem);
 	const int tid = threadIdx.x;
+	__shared__ int sNext;
 	const int R = a.counters[3];
 	sort_setup<VM>(sm);
 	unsigned phase = 0;
-	for(int r = blockIdx.x; r < R; r += gridDim.x) {
+	// Ranges differ in size: each CTA draws the next one when done.
+	for(;;) {
+		if(tid == 0) sNext = atomicAdd(&a.counters[a.work], 1);
+		__syncthreads();
+		const int r = sNext;
+		if(r >= R) break;
 		const long long begin = a.rangeBegin[r];
 		const long long end = a.rangeEnd[r];
 		const long long segStart = a.offsets[a.rangeSeg[r]];
@@ -1286,98 +1309,146 @@ struct SmallSortArgs {
 	PassPlan plan;
 	const int* offsets;
 	const int* list;
-	const int* counters;
+	int* counters;
 	int listIndex;                  // counters[listIndex] = list length
+	int work;                       // counters[work]: next list entry
 	int numArrays;                  // value arrays to permute (0 in index mode)
 	int indexMode;
 };
 
+// One segment [begin, begin + len) of at most kSmallThreads * IPT elements,
+// sorted whole in shared memory: keys and their segment-local positions go
+// through every pass, then keys are written out and each value array is
+// permuted through shared memory by the final positions (index mode writes
+// the positions). Ends with a barrier.
 template<int IPT>
-__global__ void __launch_bounds__(kSmallThreads) small_sort_kernel(const SmallSortArgs a) {
+__device__ __forceinline__ void small_sort_segment(const SmallSortArgs& a, int begin,
+	int len, unsigned* sKeys, unsigned* sIdx, unsigned* sWarpHist, unsigned* sScan,
+	unsigned ltMask, const unsigned (&nClear)[4]) {
 	constexpr int NT = kSmallThreads;
 	constexpr int TILE = NT * IPT;
 	constexpr int NW = NT / 32;
-	__shared__ unsigned sKeys[TILE];
-	__shared__ unsigned sIdx[TILE];
-	__shared__ unsigned sWarpHist[NW * kDigitBins];
-	__shared__ unsigned sScan[32];
-
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
 	const int warpBase = warp * 32 * IPT;
+
+	for(int j = tid; j < TILE; j += NT) {
+		sKeys[j] = j < len ? a.buf.keysIn[begin + j] : 0xffffffffu;
+		sIdx[j] = j;
+	}
+	for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
+	__syncthreads();
+
+	for(int p = 0; p < a.plan.numPasses; ++p) {
+		const DigitOf<false> digit(a.plan.shift[p], a.plan.width[p]);
+		unsigned rank[IPT];
+		rank_tile<IPT, false, false>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
+			lane, len, digit, ltMask, nClear, rank);
+		__syncthreads();
+		unsigned c[NW];
+		unsigned tileTotal = 0;
+#pragma unroll
+		for(int w = 0; w < NW; ++w) {
+			c[w] = sWarpHist[w * kDigitBins + tid];
+			tileTotal += c[w];
+		}
+		const unsigned incl = warp_inclusive_scan(tileTotal, lane);
+		if(lane == 31) sScan[warp] = incl;
+		__syncthreads();
+		unsigned prefix = 0;
+		for(int w = 0; w < warp; ++w) prefix += sScan[w];
+		unsigned run = prefix + incl - tileTotal;
+#pragma unroll
+		for(int w = 0; w < NW; ++w) {
+			sWarpHist[w * kDigitBins + tid] = run;
+			run += c[w];
+		}
+		unsigned keys[IPT], idx[IPT];
+#pragma unroll
+		for(int j = 0; j < IPT; ++j) {
+			keys[j] = sKeys[warpBase + j * 32 + lane];
+			idx[j] = sIdx[warpBase + j * 32 + lane];
+		}
+		__syncthreads();
+#pragma unroll
+		for(int j = 0; j < IPT; ++j) {
+			const unsigned pos = (rank[j] & 0xffffu)
+				+ sWarpHist[warp * kDigitBins + (rank[j] >> 16)];
+			sKeys[pos] = keys[j];
+			sIdx[pos] = idx[j];
+		}
+		__syncthreads();
+		for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
+		__syncthreads();
+	}
+
+	for(int j = tid; j < len; j += NT) {
+		a.buf.keysOut[begin + j] = sKeys[j];
+		if(a.indexMode) a.buf.valsOut[0][begin + j] = sIdx[j];
+	}
+	for(int v = 0; v < a.numArrays; ++v) {
+		// Stage the segment's values (the input may be the output buffer).
+		__syncthreads();
+		for(int j = tid; j < len; j += NT) sKeys[j] = a.buf.valsIn[v][begin + j];
+		__syncthreads();
+		for(int j = tid; j < len; j += NT) a.buf.valsOut[v][begin + j] = sKeys[sIdx[j]];
+	}
+	__syncthreads();
+}
+
+// Segments of at most kSmallThreads * MAXIPT elements, persistent over a
+// list (each CTA draws the next entry when done). Each segment is sorted in
+// the smallest tile of 2, 4, 8 or 16 keys per thread that holds it, so the
+// ranking work follows the segment's size.
+template<int MAXIPT>
+__global__ void __launch_bounds__(kSmallThreads) small_sort_kernel(const SmallSortArgs a) {
+	constexpr int NT = kSmallThreads;
+	constexpr int NW = NT / 32;
+	__shared__ unsigned sKeys[NT * MAXIPT];
+	__shared__ unsigned sIdx[NT * MAXIPT];
+	__shared__ unsigned sWarpHist[NW * kDigitBins];
+	__shared__ unsigned sScan[32];
+	__shared__ int sNext;
+
+	const int tid = threadIdx.x;
+	const int lane = tid & 31;
 	const unsigned ltMask = lanemask_lt();
 	unsigned nClear[4];
 #pragma unroll
 	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
 	const int count = a.counters[a.listIndex];
 
-	for(int i = blockIdx.x; i < count; i += gridDim.x) {
+	for(;;) {
+		if(tid == 0) sNext = atomicAdd(&a.counters[a.work], 1);
+		__syncthreads();
+		const int i = sNext;
+		if(i >= count) break;
 		const int s = a.list[i];
 		const int begin = a.offsets[s];
 		const int len = a.offsets[s + 1] - begin;
-		for(int j = tid; j < TILE; j += NT) {
-			sKeys[j] = j < len ? a.buf.keysIn[begin + j] : 0xffffffffu;
-			sIdx[j] = j;
-		}
-		for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
-		__syncthreads();
-
-		for(int p = 0; p < a.plan.numPasses; ++p) {
-			const DigitOf<false> digit(a.plan.shift[p], a.plan.width[p]);
-			unsigned rank[IPT];
-			rank_tile<IPT, false, false>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
-				lane, len, digit, ltMask, nClear, rank);
-			__syncthreads();
-			unsigned c[NW];
-			unsigned tileTotal = 0;
-#pragma unroll
-			for(int w = 0; w < NW; ++w) {
-				c[w] = sWarpHist[w * kDigitBins + tid];
-				tileTotal += c[w];
+		if constexpr(MAXIPT >= 16) {
+			if(len > 8 * NT) {
+				small_sort_segment<16>(a, begin, len, sKeys, sIdx, sWarpHist, sScan,
+					ltMask, nClear);
+				continue;
 			}
-			const unsigned incl = warp_inclusive_scan(tileTotal, lane);
-			if(lane == 31) sScan[warp] = incl;
-			__syncthreads();
-			unsigned prefix = 0;
-			for(int w = 0; w < warp; ++w) prefix += sScan[w];
-			unsigned run = prefix + incl - tileTotal;
-#pragma unroll
-			for(int w = 0; w < NW; ++w) {
-				sWarpHist[w * kDigitBins + tid] = run;
-				run += c[w];
-			}
-			unsigned keys[IPT], idx[IPT];
-#pragma unroll
-			for(int j = 0; j < IPT; ++j) {
-				keys[j] = sKeys[warpBase + j * 32 + lane];
-				idx[j] = sIdx[warpBase + j * 32 + lane];
-			}
-			__syncthreads();
-#pragma unroll
-			for(int j = 0; j < IPT; ++j) {
-				const unsigned pos = (rank[j] & 0xffffu)
-					+ sWarpHist[warp * kDigitBins + (rank[j] >> 16)];
-				sKeys[pos] = keys[j];
-				sIdx[pos] = idx[j];
-			}
-			__syncthreads();
-			for(int j = tid; j < NW * kDigitBins; j += NT) sWarpHist[j] = 0;
-			__syncthreads();
 		}
-
-		for(int j = tid; j < len; j += NT) {
-			a.buf.keysOut[begin + j] = sKeys[j];
-			if(a.indexMode) a.buf.valsOut[0][begin + j] = sIdx[j];
+		if constexpr(MAXIPT >= 8) {
+			if(len > 4 * NT) {
+				small_sort_segment<8>(a, begin, len, sKeys, sIdx, sWarpHist, sScan,
+					ltMask, nClear);
+				continue;
+			}
 		}
-		for(int v = 0; v < a.numArrays; ++v) {
-			// Stage the segment's values (the input may be the output buffer).
-			__syncthreads();
-			for(int j = tid; j < len; j += NT) sKeys[j] = a.buf.valsIn[v][begin + j];
-			__syncthreads();
-			for(int j = tid; j < len; j += NT) a.buf.valsOut[v][begin + j] = sKeys[sIdx[j]];
+		if constexpr(MAXIPT >= 4) {
+			if(len > 2 * NT) {
+				small_sort_segment<4>(a, begin, len, sKeys, sIdx, sWarpHist, sScan,
+					ltMask, nClear);
+				continue;
+			}
 		}
-		__syncthreads();
+		small_sort_segment<2>(a, begin, len, sKeys, sIdx, sWarpHist, sScan, ltMask, nClear);
 	}
 }
 
@@ -1562,7 +1633,7 @@ cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
 		failTile, hostError, numSMs, stream);
 }
 
-// Segmented scratch: [counters 8][lists 5 x S][range table 4 x Rmax]
+// Segmented scratch: [counters][lists 5 x S][range table 4 x Rmax]
 // [counts Rmax x 256][rangeStart Rmax x 256], in 32-bit words.
 struct SegScratch {
 	int* counters;
@@ -1579,14 +1650,24 @@ struct SegScratch {
 	unsigned* rangeStart;
 };
 
+// The smallest tile of any value mode: the most ranges a plan can cut.
+constexpr int kMinTile = std::min({SortLayout<-1>::TILE, SortLayout<0>::TILE,
+	SortLayout<1>::TILE, SortLayout<2>::TILE, SortLayout<3>::TILE, SortLayout<4>::TILE,
+	SortLayout<5>::TILE, SortLayout<6>::TILE});
+
+// Ranges of a plan: a large segment (more than 4096 elements) of t tiles gets
+// min(64, ceil(t / 4)) ranges, and t <= len / tile + 2 (aligned-down start,
+// partial end), so it gets at most len / (4 tile) + 1.25. Summed over at most
+// n / 4096 large segments that is below n / tile + numSegments for any tile
+// up to 7680 keys (0.25 n / 4096 <= 0.75 n / tile).
 static size_t seg_max_ranges(int n, int numSegments) {
-	return (size_t)n / SortLayout<2>::TILE + (size_t)numSegments + 1;
+	return (size_t)n / kMinTile + (size_t)numSegments + 1;
 }
 
 size_t seg_scratch_bytes(int n, int numSegments) {
 	const size_t S = (size_t)numSegments;
 	const size_t R = seg_max_ranges(n, numSegments);
-	return sizeof(unsigned) * (8 + 5 * S + 4 * R + 2 * R * kDigitBins) + 256;
+	return sizeof(unsigned) * (kSegCounters + 5 * S + 4 * R + 2 * R * kDigitBins) + 256;
 }
 
 static SegScratch seg_scratch(void* base, int n, int numSegments) {
@@ -1594,7 +1675,7 @@ static SegScratch seg_scratch(void* base, int n, int numSegments) {
 	const size_t R = seg_max_ranges(n, numSegments);
 	unsigned* w = static_cast<unsigned*>(base);
 	SegScratch x;
-	x.counters = reinterpret_cast<int*>(w); w += 8;
+	x.counters = reinterpret_cast<int*>(w); w += kSegCounters;
 	x.tinyList = reinterpret_cast<int*>(w); w += S;
 	x.smallList = reinterpret_cast<int*>(w); w += S;
 	x.largeList = reinterpret_cast<int*>(w); w += S;
@@ -1646,10 +1727,12 @@ cudaError_t launch_seg_small(const PassBuffers& buf, int valueMode,
 	a.indexMode = valueMode == kValueIndex;
 	a.list = x.tinyList;
 	a.listIndex = 0;
+	a.work = kSegWorkSmall;
 	small_sort_kernel<kSegTinyMax / kSmallThreads><<<numSMs * 8, kSmallThreads, 0,
 		stream>>>(a);
 	a.list = x.smallList;
 	a.listIndex = 1;
+	a.work = kSegWorkSmall + 1;
 	small_sort_kernel<kSegSmallMax / kSmallThreads><<<numSMs * 4, kSmallThreads, 0,
 		stream>>>(a);
 	return cudaGetLastError();
@@ -1691,6 +1774,7 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	c.width = plan.width[pass];
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
 	c.counts = x.counts;
+	c.work = kSegWork + 2 * pass;
 	seg_count_kernel<<<numSMs * 4, kCountThreads, 0, stream>>>(c);
 
 	SegScanArgs q;
@@ -1720,6 +1804,7 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	a.rangeEnd = x.rangeEnd;
 	a.rangeSeg = x.rangeSeg;
 	a.counters = x.counters;
+	a.work = kSegWork + 2 * pass + 1;
 	a.rangeStart = x.rangeStart;
 	a.rangeTrivial = x.rangeTrivial;
 	switch(valueMode) {
