@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--workload", default="pairs_and24_32M",
                    choices=sorted(workloads.WORKLOADS) + ["served", "bwt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--server-slots", type=int, default=4,
+                   help="served workload: server slots (engine + stream each)")
     p.add_argument("--bwt-bytes", type=int, default=8 << 20,
                    help="bwt workload: block size in bytes")
     p.add_argument("--bwt-key", type=int, default=16,
@@ -786,7 +788,7 @@ def run_served(args, device, local):
     serial(np.zeros(R))                       # warm-up
     lat0, span0 = serial(np.zeros(R))
     capacity = R / span0                      # requests per second
-    server = api.SortServer(memory_budget=args.server_budget << 30, slots=4,
+    server = api.SortServer(memory_budget=args.server_budget << 30, slots=args.server_slots,
                             coalesce_max=1 << 20)
     served(np.zeros(R), server)               # warm-up: grows the memory pool
     results = []
@@ -815,7 +817,7 @@ def run_served(args, device, local):
                        "sizes": "log-uniform [1024, 16777216]",
                        "mix": "50% keys-only / 50% key+value, endBit in {16, 24, 32}",
                        "arrivals": "Poisson at 0.5/0.8/1.0 x serial capacity",
-                       "memory_budget_GiB": args.server_budget,
+                       "memory_budget_GiB": args.server_budget, "slots": args.server_slots,
                        "elements": total_elems, "parallelism": "replicas1"},
             "e2e": {"value": round(best, 1), "unit": UNIT,
                     "h2d_bytes_per_step": int(4 * (sizes + sizes * has_values).sum() / R),

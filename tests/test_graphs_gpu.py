@@ -113,3 +113,26 @@ def test_graphs_off_and_shape_changes(fresh_engine, oracle_mod):
             assert np.array_equal(ds.result()[0], ek)
         if not enable:
             assert fresh_engine.graph_stats()[1] == 0
+
+
+def test_typed_sort_replays_graph(fresh_engine, oracle_mod):
+    """sortArrayTyped (float keys) repeated on the same buffers: the key
+    transforms are part of the captured sequence."""
+    import torch
+    n = 70_000
+    ds = DeviceSort(np.zeros(n, np.uint32), [np.zeros(n, np.uint32)], 1, 0, 32)
+    rng = np.random.default_rng(5)
+    for it in range(5):
+        f = (rng.standard_normal(n) * 1e3).astype(np.float32)
+        keys = f.view(np.uint32).copy()
+        vals = np.arange(n, dtype=np.uint32)
+        load_inputs(ds, keys, [vals])
+        torch.cuda.synchronize()
+        assert fresh_engine.sort_array_typed(ds.data, api.KEY_FLOAT32) == 0
+        assert fresh_engine.synchronize() == 0
+        torch.cuda.synchronize()
+        k, (v,) = ds.result()
+        order = np.argsort(f, kind="stable")
+        assert np.array_equal(v, order.astype(np.uint32))
+        assert np.array_equal(k, keys[order])
+    assert fresh_engine.graph_stats()[0] >= 3
