@@ -32,8 +32,9 @@ int SORTAPI sortPlanPasses(int firstBit, int endBit, int bitPass,
 	int* widths);
 
 /* Fault injection for tests of the device-side bounded waits: in the next
- * pass launched by this engine, the CTA that sorts tile `tile` (7680 or 7168
- * elements each) also waits on a barrier that nothing completes, so that
+ * pass launched by this engine, the CTA that sorts tile `tile` (tiles of the
+ * value mode's shape in tile_config.h: 5120, 7680 or 6144 elements as
+ * shipped) also waits on a barrier that nothing completes, so that
  * bounded wait runs out (about half a second) and the sort reports
  * SORT_STATUS_KERNEL_ERROR through sortSynchronize. -1 turns it off. Nothing
  * faults, traps or hangs; the engine is usable afterwards. */

@@ -32,8 +32,9 @@ def layout(rng, sizes):
 
 
 LAYOUTS = {
-    "edges": [0, 1, 2, 511, 512, 513, 4095, 4096, 4097, 0, 7167, 7168, 7169, 7680,
-              7681, 15361, 30000, 100003, 3],
+    "edges": [0, 1, 2, 511, 512, 513, 1023, 1024, 1025, 2047, 2048, 2049, 4095, 4096,
+              4097, 0, 5119, 5120, 5121, 6143, 6144, 6145, 7167, 7168, 7169, 7680, 7681,
+              15361, 30000, 100003, 3],
     "one_big": [250_001],
     "many_tiny": [int(x) for x in np.random.default_rng(1).integers(0, 40, 3000)],
     "lognormal": [int(x) for x in np.clip(np.rint(

@@ -39,10 +39,11 @@ def test_golden_fixtures(engine, path):
     assert_same(ds, z["expect_keys"], [z[f"expect_values{i}"] for i in range(arrays)])
 
 
-# Around the tile sizes of the sort kernel (7680 for keys, indices and one
-# value array; 7168 for several value arrays) and of older shapes.
-SIZES = [1, 2, 31, 255, 4095, 4097, 7167, 7168, 7169, 7679, 7680, 7681, 15361,
-         100003]
+# Around the tile sizes of the sort kernel with the shipped tile shapes
+# (5120 keys only, 7680 indices or one value array, 6144 several value
+# arrays), two tiles, and of other shapes the autotuner may pick.
+SIZES = [1, 2, 31, 255, 4095, 4097, 5119, 5120, 5121, 6143, 6144, 6145, 7167, 7168,
+         7169, 7679, 7680, 7681, 10241, 12289, 15361, 100003]
 
 
 @pytest.mark.parametrize("n", SIZES)
