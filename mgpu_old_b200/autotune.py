@@ -6,7 +6,10 @@
 
 A candidate is one assignment of tile_config.h's values for one class:
 "keys" (keys only), "single" (index mode, one value array), "multi" (two to
-six value arrays) or "digits" (the widest digit of sortArray's pass plan). Each
+six value arrays), "digits" (the widest digit of sortArray's pass plan), or
+"<class>_ballot" (how many digit bits the warp ranking of that class resolves
+by ballots, the rest by match.any; "small" is the segmented sort's kernel for
+segments that fit one tile). Each
 candidate is a separate build of the library (build_variant, under
 _build/tune/), because tile shapes are compile-time constants of the
 kernels. The build step runs anywhere nvcc does; the measure step loads each
@@ -54,6 +57,36 @@ CLASSES = {
         "candidates": [(8,), (7,), (6,)],
         "workloads": [("pairs_and24", 1 << 25), ("keys_u32", 1 << 24)],
     },
+    # How the warp ranking finds the lanes sharing a digit: ballots on the
+    # low 8, 5 or 4 digit bits, match.any on the rest (match_digit8).
+    "keys_ballot": {
+        "keys": ("MGPU_SORT_KEYS_BALLOT_BITS",),
+        "candidates": [(8,), (5,), (4,)],
+        "workloads": [("keys_u32", 1 << 24), ("keys_u32", 1 << 26)],
+    },
+    "single_ballot": {
+        "keys": ("MGPU_SORT_SINGLE_BALLOT_BITS",),
+        "candidates": [(8,), (5,), (4,)],
+        "workloads": [("pairs_and24", 1 << 25), ("pairs_u32", 1 << 24), ("index_u32", 1 << 24),
+                      ("segments_lognormal", 10_000)],
+    },
+    # The same choice for sortArray calls of MGPU_SORT_SINGLE_LARGE_ELEMENTS
+    # keys or more.
+    "single_large_ballot": {
+        "keys": ("MGPU_SORT_SINGLE_LARGE_BALLOT_BITS",),
+        "candidates": [(8,), (5,), (4,)],
+        "workloads": [("pairs_u32", 1 << 26), ("pairs_u32", 3 << 25), ("index_u32", 1 << 26)],
+    },
+    "multi_ballot": {
+        "keys": ("MGPU_SORT_MULTI_BALLOT_BITS",),
+        "candidates": [(8,), (5,), (4,)],
+        "workloads": [("multi6_17bit", 1 << 24), ("multi3_u32", 1 << 24)],
+    },
+    "small_ballot": {
+        "keys": ("MGPU_SORT_SMALL_BALLOT_BITS",),
+        "candidates": [(8,), (5,), (4,)],
+        "workloads": [("segments_small", 50_000)],
+    },
 }
 
 
@@ -99,6 +132,21 @@ def make_case(kind: str, n: int):
         return c
     if kind == "multi6_17bit":
         return workloads.multi6_17bit(n)
+    if kind == "segments_lognormal":
+        return workloads.segments_lognormal(n)
+    if kind == "segments_small":
+        # Many short segments (median 256): the small-segment kernel's work.
+        import numpy as np
+        sizes = np.clip(np.rint(np.random.default_rng(12).lognormal(np.log(256.0), 1.0, n)),
+                        1, 4096).astype(np.int64)
+        offsets = np.zeros(n + 1, np.int64)
+        np.cumsum(sizes, out=offsets[1:])
+        total = int(offsets[-1])
+        keys = np.random.default_rng(13).integers(0, 1 << 32, total, dtype=np.uint64)
+        local = (np.arange(total, dtype=np.int64) - np.repeat(offsets[:-1], sizes))
+        return workloads.SegmentedCase(f"segments_small_{n}", keys.astype(np.uint32),
+                                       [local.astype(np.uint32)], 1, 0, 32,
+                                       offsets=offsets.astype(np.int32))
     if kind == "multi3_u32":
         import numpy as np
         rng = np.random.Generator(np.random.MT19937(9))
@@ -109,10 +157,71 @@ def make_case(kind: str, n: int):
     raise ValueError(kind)
 
 
+def check_segmented(case, keys, local) -> None:
+    """Exact check of a segmented sort whose value array holds each key's
+    position within its segment: every segment's keys are its input keys
+    ordered stably (ties keep input order)."""
+    import numpy as np
+    sizes = np.diff(case.offsets.astype(np.int64))
+    seg = np.repeat(np.arange(sizes.size), sizes)
+    order = np.lexsort((case.keys, seg))      # stable within equal keys
+    if not np.array_equal(keys, case.keys[order]):
+        raise RuntimeError(f"{case.name}: keys differ from a stable per-segment sort")
+    start = case.offsets[:-1].astype(np.int64)
+    if not np.array_equal(local.astype(np.int64) + np.repeat(start, sizes), order):
+        raise RuntimeError(f"{case.name}: positions differ from a stable per-segment sort")
+
+
+def time_segmented(case, steps: int) -> float:
+    """Median ms of `steps` sortSegmentedArray calls on the case, after an
+    exact check of the result."""
+    import numpy as np
+    import torch
+    from mgpu_old_b200 import api
+    dev = torch.device("cuda", 0)
+    n = case.n
+    cap = (n + 2047) // 2048 * 2048
+    src_k = torch.zeros(cap, dtype=torch.int32, device=dev)
+    src_v = torch.zeros(cap, dtype=torch.int32, device=dev)
+    src_k[:n] = torch.from_numpy(case.keys.view(np.int32)).to(dev)
+    src_v[:n] = torch.from_numpy(case.values[0].view(np.int32)).to(dev)
+    offs = torch.from_numpy(case.offsets.astype(np.int32)).to(dev)
+    k = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(2)]
+    v = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(2)]
+    d = api.SortData()
+    d.maxElements, d.numElements, d.valueCount = cap, n, 1
+    d.firstBit, d.endBit = case.first_bit, case.end_bit
+    d.keys[0], d.keys[1] = k[0].data_ptr(), k[1].data_ptr()
+    d.values[0][0], d.values[0][1] = v[0].data_ptr(), v[1].data_ptr()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    eng = api.MgpuSort()
+    times = []
+    for it in range(steps + 3):
+        k[0].copy_(src_k)
+        v[0].copy_(src_v)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        api.check(eng.sort_segmented(d, offs.data_ptr(), case.num_segments))
+        e1.record()
+        e1.synchronize()
+        if it >= 3:
+            times.append(e0.elapsed_time(e1))
+    api.check(eng.synchronize())
+    check_segmented(case, k[0][:n].cpu().numpy().view(np.uint32),
+                    v[0][:n].cpu().numpy().view(np.uint32))
+    eng.release()
+    return sorted(times)[len(times) // 2]
+
+
 def time_case(case, steps: int) -> float:
     """Median ms of `steps` sorts of the case through sortArray, after a
     check of the result (the first value array, when it holds the input
     positions, must gather the input keys into the sorted output)."""
+    from mgpu_old_b200 import workloads
+    if isinstance(case, workloads.SegmentedCase):
+        return time_segmented(case, steps)
     import numpy as np
     import torch
     from mgpu_old_b200 import api
@@ -237,24 +346,40 @@ def cmd_write(args) -> int:
     header = args.header or CONFIG_H
     with open(header) as f:
         text = f.read()
-    table_lines = ["// Measured by the autotuner (median ms per sort; score = geometric",
-                   "// mean of time / best time over the class's workloads):"]
+    import re
+    # The table already in the header, one block of lines per class: blocks
+    # of classes measured again are replaced, the others kept.
+    blocks = {}
+    start = text.find("// Measured by the autotuner")
+    if start >= 0:
+        end = text.find("#pragma once")
+        cls = None
+        for line in text[start:end].splitlines():
+            m = re.match(r"//   (\w+): chosen ", line)
+            if m:
+                cls = m.group(1)
+                blocks[cls] = []
+            if cls:
+                blocks[cls].append(line)
+        text = text[:start] + text[end:]
     for cls, table in results.items():
         if not table:
             continue
         winner, scores = choose(table)
         for key, val in zip(CLASSES[cls]["keys"], winner.split("x")):
-            import re
             text = re.sub(rf"#define {key} \d+", f"#define {key} {val}", text)
-        table_lines.append(f"//   {cls}: chosen {winner}")
+        lines = [f"//   {cls}: chosen {winner}"]
         for cand, t in sorted(table.items(), key=lambda kv: scores.get(kv[0], 9)):
             cells = ", ".join(f"{w} {ms:.3f}" for w, ms in sorted(t.items()))
-            table_lines.append(f"//     {cand:>10}  score {scores.get(cand, float('nan')):.3f}  "
-                               f"{cells}")
-    start = text.find("// Measured by the autotuner")
-    if start >= 0:
-        end = text.find("#pragma once")
-        text = text[:start] + text[end:]
+            lines.append(f"//     {cand:>10}  score {scores.get(cand, float('nan')):.3f}  "
+                         f"{cells}")
+        blocks[cls] = lines
+    table_lines = ["// Measured by the autotuner (median ms per sort; score = geometric",
+                   "// mean of time / best time over the class's workloads):"]
+    for cls in CLASSES:
+        table_lines += blocks.pop(cls, [])
+    for lines in blocks.values():
+        table_lines += lines
     text = text.replace("#pragma once", "\n".join(table_lines) + "\n#pragma once", 1)
     with open(header, "w") as f:
         f.write(text)

@@ -33,7 +33,8 @@ namespace mgpusort {
 // passes are launched so that each may be scheduled while its predecessor
 // in the stream drains. Each waits (griddepcontrol.wait) for the
 // predecessor to complete, with its memory visible, before touching global
-// memory, and then lets its own successor launch. Launched without the
+// memory. Count and scan then let their successor launch at once; the sort
+// kernel releases its successor when it exits. Launched without the
 // attribute (or after a non-kernel stream operation) the wait returns at
 // once.
 __device__ __forceinline__ void wait_for_predecessor() {
@@ -389,6 +390,13 @@ template<int VM> struct SortConfig {
 		: VM == 0 ? MGPU_SORT_KEYS_ITEMS : MGPU_SORT_SINGLE_ITEMS;
 	static constexpr int kMinBlocks = VM >= 2 ? MGPU_SORT_MULTI_MIN_BLOCKS
 		: VM == 0 ? MGPU_SORT_KEYS_MIN_BLOCKS : MGPU_SORT_SINGLE_MIN_BLOCKS;
+	// Digit bits resolved by ballots in the warp ranking (match_digit8);
+	// sortArray on at least kLargeElements keys uses kBallotBitsLarge.
+	static constexpr int kBallotBits = VM >= 2 ? MGPU_SORT_MULTI_BALLOT_BITS
+		: VM == 0 ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_BALLOT_BITS;
+	static constexpr int kBallotBitsLarge = VM >= 2 ? MGPU_SORT_MULTI_BALLOT_BITS
+		: VM == 0 ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_LARGE_BALLOT_BITS;
+	static constexpr int kLargeElements = MGPU_SORT_SINGLE_LARGE_ELEMENTS;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
@@ -422,33 +430,48 @@ template<int VM> struct SortLayout {
 };
 
 // Peers of an 8-bit digit: the lanes of the warp whose digit equals this
-// lane's. From the eight ballots of the digit bits, lane l builds two
-// entries of two 16-entry tables: the lanes whose low nibble is l & 15 and
-// the lanes whose high nibble is l & 15 (nClear[k] is all ones where bit k of
-// l & 15 is clear, so ballot ^ nClear[k] is the set of lanes agreeing with
-// that bit). A lane's peers are the AND of the low-table entry for its low
-// nibble and the high-table entry for its high nibble, fetched by shuffle.
+// lane's. The low BB bits of the digit are resolved by ballots and a lookup
+// table spread over the lanes: from the ballots of bits 0..3, lane l builds
+// the entry for low nibble l & 15, the set of lanes whose low nibble equals
+// it (nClear[k] is all ones where bit k of lane l is clear, so
+// ballot ^ nClear[k] is the set of lanes agreeing with that bit of l), and a
+// lane fetches the entry of its own nibble by shuffle. The remaining high
+// bits are resolved in one of two ways:
+//   BB = 8: four more ballots build a second 16-entry table for the high
+//           nibble; peers = low entry & high entry (two shuffles);
+//   BB = 5: a fifth ballot widens the table to 32 entries (bit 4 of the
+//           lane), and match.any on the top three bits gives the rest;
+//   BB = 4: match.any on the high nibble.
+// All three return the same set; which is fastest depends on the tile shape
+// and is a choice of the autotuner.
+template<int BB>
 __device__ __forceinline__ unsigned match_digit8(unsigned d,
 	const unsigned (&nClear)[4]) {
-	unsigned bal[8];
+	static_assert(BB == 4 || BB == 5 || BB == 8, "ballot bits: 4, 5 or 8");
+	unsigned lo = __ballot_sync(0xffffffffu, d & 1u) ^ nClear[0];
 #pragma unroll
-	for(int b = 0; b < 8; ++b) bal[b] = __ballot_sync(0xffffffffu, d & (1u << b));
-	unsigned lo = bal[0] ^ nClear[0];
-	unsigned hi = bal[4] ^ nClear[0];
+	for(int k = 1; k < 4; ++k) lo &= __ballot_sync(0xffffffffu, d & (1u << k)) ^ nClear[k];
+	if constexpr(BB == 8) {
+		unsigned hi = __ballot_sync(0xffffffffu, d & 16u) ^ nClear[0];
 #pragma unroll
-	for(int k = 1; k < 4; ++k) {
-		lo &= bal[k] ^ nClear[k];
-		hi &= bal[4 + k] ^ nClear[k];
+		for(int k = 1; k < 4; ++k) hi &= __ballot_sync(0xffffffffu, d & (16u << k)) ^ nClear[k];
+		return __shfl_sync(0xffffffffu, lo, d & 15u) & __shfl_sync(0xffffffffu, hi, d >> 4);
+	} else if constexpr(BB == 5) {
+		const unsigned nClear4 = (threadIdx.x & 16u) ? 0u : 0xffffffffu;
+		lo &= __ballot_sync(0xffffffffu, d & 16u) ^ nClear4;
+		return __match_any_sync(0xffffffffu, d >> 5) & __shfl_sync(0xffffffffu, lo, d & 31u);
+	} else {
+		return __match_any_sync(0xffffffffu, d >> 4) & __shfl_sync(0xffffffffu, lo, d & 15u);
 	}
-	return __shfl_sync(0xffffffffu, lo, d & 15u) & __shfl_sync(0xffffffffu, hi, d >> 4);
 }
 
 // Stable warp rank of one item: the group of peers starts at the warp's
 // running count of the digit, which the highest peer then advances by the
 // group's size. Returns (digit << 16) | rank within the warp.
+template<int BB>
 __device__ __forceinline__ unsigned rank_item(unsigned d, unsigned* warpHist,
 	int lane, unsigned ltMask, const unsigned (&nClear)[4]) {
-	const unsigned peers = match_digit8(d, nClear);
+	const unsigned peers = match_digit8<BB>(d, nClear);
 	// Every peer reads the count; the highest peer then adds the group.
 	const unsigned base = warpHist[d];
 	__syncwarp();
@@ -481,7 +504,7 @@ template<bool BYTE> struct DigitOf {
 // tile element w*32*IPT + i*32 + l, so (item, lane) order is input order per
 // warp). In a partial tile the elements past `count` get digit 255: they
 // rank after every real key and are never stored.
-template<int IPT, bool FULL, bool BYTE>
+template<int IPT, bool FULL, bool BYTE, int BB>
 __device__ __forceinline__ void rank_tile(const unsigned* sKeys, unsigned* myHist,
 	int warpBase, int lane, int count, const DigitOf<BYTE>& digit, unsigned ltMask,
 	const unsigned (&nClear)[4], unsigned (&rank)[IPT]) {
@@ -490,7 +513,7 @@ __device__ __forceinline__ void rank_tile(const unsigned* sKeys, unsigned* myHis
 		const int idx = warpBase + i * 32 + lane;
 		unsigned d = digit(sKeys[idx]);
 		if(!FULL && idx >= count) d = kDigitBins - 1;
-		rank[i] = rank_item(d, myHist, lane, ltMask, nClear);
+		rank[i] = rank_item<BB>(d, myHist, lane, ltMask, nClear);
 	}
 }
 
@@ -631,7 +654,7 @@ __device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int co
 // copied in while a tile is sorted (two key slots), its value array as soon
 // as this tile has stored its own. Index mode writes position - indexBase.
 // Requires sort_setup and a barrier before.
-template<int VM, bool BYTE>
+template<int VM, bool BYTE, int BB>
 __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 	long long begin, long long end, long long indexBase, unsigned& phase) {
 	static_assert(VM <= 1, "one value array at most");
@@ -695,7 +718,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 			if(!mbar_wait_bounded(&sBar[slot], (phase >> slot) & 1u))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 			phase ^= 1u << slot;
-			rank_tile<IPT, true, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			// Plain loads (a partial tile, or data that is not 16-byte
@@ -706,7 +729,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 					sVals[i] = i < count ? a.buf.valsIn[0][tileStart + i] : 0u;
 			}
 			__syncthreads();
-			rank_tile<IPT, false, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -805,7 +828,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 // tile's keys are requested as soon as this tile's keys are stored. Tiles
 // without bulk copies gather their values from global memory (a window of
 // one tile).
-template<int VM, bool BYTE>
+template<int VM, bool BYTE, int BB>
 __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 	long long begin, long long end, unsigned& phase) {
 
@@ -865,13 +888,13 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 		unsigned rank[IPT];
 		if(bulk) {
 			wait_bar(0);
-			rank_tile<IPT, true, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			for(int i = tid; i < TILE; i += NT)
 				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
 			__syncthreads();
-			rank_tile<IPT, false, BYTE>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -949,21 +972,23 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 	}
 }
 
-template<int VM, bool BYTE>
+template<int VM, bool BYTE, int BB>
 __device__ __forceinline__ void sort_range(const SortArgs& a, const SortSmem<VM>& sm,
 	long long begin, long long end, long long indexBase, unsigned& phase) {
-	if constexpr(VM >= 2) sort_range_multi<VM, BYTE>(a, sm, begin, end, phase);
-	else sort_range_single<VM, BYTE>(a, sm, begin, end, indexBase, phase);
+	if constexpr(VM >= 2) sort_range_multi<VM, BYTE, BB>(a, sm, begin, end, phase);
+	else sort_range_single<VM, BYTE, BB>(a, sm, begin, end, indexBase, phase);
 }
 
 // One pass over a whole array: CTA r sorts range r of the split.
-template<int VM, bool BYTE>
+template<int VM, bool BYTE, int BB>
 __global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
 sort_kernel(const SortArgs a) {
 	using L = SortLayout<VM>;
 	extern __shared__ __align__(128) unsigned smem[];
+	// The successor (the next pass's count) is released when this grid
+	// exits, not here: released early, its CTAs cost more than the launch
+	// latency they hide.
 	wait_for_predecessor();
-	allow_successor();
 	const SortSmem<VM> sm(smem);
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
@@ -991,7 +1016,7 @@ sort_kernel(const SortArgs a) {
 	sort_setup<VM>(sm);
 	__syncthreads();
 	unsigned phase = 0;
-	sort_range<VM, BYTE>(a, sm, begin, end, 0, phase);
+	sort_range<VM, BYTE, BB>(a, sm, begin, end, 0, phase);
 }
 
 ////////////////////////////////////////////////////////////////////////////////
@@ -1293,7 +1318,8 @@ seg_sort_kernel(const SegSortArgs a) {
 		const bool trivial = a.rangeTrivial[r] != 0;
 		__syncthreads();
 		if(trivial) copy_range<VM>(a.sort, begin, end, segStart);
-		else sort_range<VM, BYTE>(a.sort, sm, begin, end, segStart, phase);
+		else sort_range<VM, BYTE, SortConfig<VM>::kBallotBits>(a.sort, sm, begin, end, segStart,
+			phase);
 		__syncthreads();
 	}
 }
@@ -1303,6 +1329,7 @@ seg_sort_kernel(const SegSortArgs a) {
 // written out and each value array is permuted through shared memory by
 // the final positions (index mode writes the positions).
 constexpr int kSmallThreads = 256;
+constexpr int kSmallBallotBits = MGPU_SORT_SMALL_BALLOT_BITS;
 
 struct SmallSortArgs {
 	PassBuffers buf;                // in: [0] arrays; out: the result arrays
@@ -1343,7 +1370,7 @@ __device__ __forceinline__ void small_sort_segment(const SmallSortArgs& a, int b
 	for(int p = 0; p < a.plan.numPasses; ++p) {
 		const DigitOf<false> digit(a.plan.shift[p], a.plan.width[p]);
 		unsigned rank[IPT];
-		rank_tile<IPT, false, false>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
+		rank_tile<IPT, false, false, kSmallBallotBits>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
 			lane, len, digit, ltMask, nClear, rank);
 		__syncthreads();
 		unsigned c[NW];
@@ -1465,8 +1492,14 @@ template<int VM>
 static cudaError_t set_sort_attributes() {
 	const int bytes = (int)SortLayout<VM>::kBytes;
 	const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-	cudaError_t e = cudaFuncSetAttribute(sort_kernel<VM, false>, attr, bytes);
-	if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true>, attr, bytes);
+	constexpr int bb = SortConfig<VM>::kBallotBits;
+	constexpr int bbLarge = SortConfig<VM>::kBallotBitsLarge;
+	cudaError_t e = cudaFuncSetAttribute(sort_kernel<VM, false, bb>, attr, bytes);
+	if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true, bb>, attr, bytes);
+	if constexpr(bbLarge != bb) {
+		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, false, bbLarge>, attr, bytes);
+		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true, bbLarge>, attr, bytes);
+	}
 	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
 	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
 	return e;
@@ -1522,7 +1555,8 @@ static int sort_ctas_per_sm() {
 	static int perSM = 0;
 	if(!perSM) {
 		int v = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, sort_kernel<VM, false>,
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v,
+			sort_kernel<VM, false, SortConfig<VM>::kBallotBits>,
 			SortLayout<VM>::NT, SortLayout<VM>::kBytes);
 		perSM = v > 0 ? v : 1;
 	}
@@ -1583,14 +1617,23 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 		stream, s);
 }
 
-template<int VM>
-static cudaError_t launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
+template<int VM, int BB>
+static cudaError_t launch_sort_bb(const SortArgs& a, cudaStream_t stream) {
 	using L = SortLayout<VM>;
 	if(a.width == 8 && (a.shift & 7) == 0)
-		return launch_dependent(sort_kernel<VM, true>, a.split.numRanges, L::NT, L::kBytes,
-			stream, a);
-	return launch_dependent(sort_kernel<VM, false>, a.split.numRanges, L::NT, L::kBytes,
-		stream, a);
+		return launch_dependent(sort_kernel<VM, true, BB>, a.split.numRanges, L::NT,
+			L::kBytes, stream, a);
+	return launch_dependent(sort_kernel<VM, false, BB>, a.split.numRanges, L::NT,
+		L::kBytes, stream, a);
+}
+
+template<int VM>
+static cudaError_t launch_sort_vm(const SortArgs& a, cudaStream_t stream) {
+	using C = SortConfig<VM>;
+	if constexpr(C::kBallotBitsLarge != C::kBallotBits) {
+		if(a.n >= C::kLargeElements) return launch_sort_bb<VM, C::kBallotBitsLarge>(a, stream);
+	}
+	return launch_sort_bb<VM, C::kBallotBits>(a, stream);
 }
 
 cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,

@@ -1,13 +1,18 @@
-// Tile shapes and digit width of the sort passes.
+// Tile shapes, digit width and warp-ranking method of the sort passes.
 //
 // These values are the choices of the autotuner (mgpu_old_b200/autotune.py),
-// which builds the library once per candidate shape, times each build on a
-// B200 over a fixed set of workloads and writes this file with the fastest
-// shape per class. Every value can be overridden at build time with -D.
+// which builds the library once per candidate, times each build on a B200
+// over a fixed set of workloads and writes this file with the fastest
+// candidate per class. Every value can be overridden at build time with -D.
 //
 //  * keys: keys only (sort_range_single without values);
 //  * single: index mode or one value array (sort_range_single);
-//  * multi: two to six value arrays (sort_range_multi).
+//  * multi: two to six value arrays (sort_range_multi);
+//  * digits: the widest digit of a pass;
+//  * <class>_ballot: digit bits the warp ranking of the class resolves by
+//    ballots (match_digit8); single_large_ballot applies to sortArray calls
+//    of at least MGPU_SORT_SINGLE_LARGE_ELEMENTS keys, small_ballot to the
+//    segmented sort's kernel for segments that fit one tile.
 // Measured by the autotuner (median ms per sort; score = geometric
 // mean of time / best time over the class's workloads):
 //   keys: chosen 256x20x3
@@ -32,6 +37,26 @@
 //              8  score 1.000  keys_u32_16777216 0.397, pairs_and24_33554432 0.674
 //              7  score 1.230  keys_u32_16777216 0.481, pairs_and24_33554432 0.842
 //              6  score 1.333  keys_u32_16777216 0.565, pairs_and24_33554432 0.842
+//   keys_ballot: chosen 5
+//              5  score 1.000  keys_u32_16777216 0.367, keys_u32_67108864 1.247
+//              4  score 1.097  keys_u32_16777216 0.401, keys_u32_67108864 1.370
+//              8  score 1.121  keys_u32_16777216 0.410, keys_u32_67108864 1.403
+//   single_ballot: chosen 5
+//              5  score 1.000  index_u32_16777216 0.463, pairs_and24_33554432 0.623, pairs_u32_16777216 0.469, segments_lognormal_10000 3.916
+//              4  score 1.049  index_u32_16777216 0.496, pairs_and24_33554432 0.625, pairs_u32_16777216 0.498, segments_lognormal_10000 4.166
+//              8  score 1.068  index_u32_16777216 0.496, pairs_and24_33554432 0.668, pairs_u32_16777216 0.500, segments_lognormal_10000 4.159
+//   single_large_ballot: chosen 4
+//              4  score 1.000  index_u32_67108864 1.697, pairs_u32_100663296 2.485, pairs_u32_67108864 1.710
+//              8  score 1.007  index_u32_67108864 1.700, pairs_u32_100663296 2.522, pairs_u32_67108864 1.716
+//              5  score 1.036  index_u32_67108864 1.743, pairs_u32_100663296 2.614, pairs_u32_67108864 1.759
+//   multi_ballot: chosen 8
+//              8  score 1.001  multi3_u32_16777216 0.885, multi6_17bit_16777216 1.210
+//              5  score 1.005  multi3_u32_16777216 0.891, multi6_17bit_16777216 1.210
+//              4  score 1.006  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.225
+//   small_ballot: chosen 5
+//              5  score 1.000  segments_small_50000 1.026
+//              4  score 1.018  segments_small_50000 1.045
+//              8  score 1.054  segments_small_50000 1.081
 #pragma once
 
 #ifndef MGPU_SORT_KEYS_THREADS
@@ -60,6 +85,29 @@
 #endif
 #ifndef MGPU_SORT_MULTI_MIN_BLOCKS
 #define MGPU_SORT_MULTI_MIN_BLOCKS 1
+#endif
+// Digit bits the warp ranking resolves by ballots (8, 5 or 4); match.any
+// resolves the rest. Keys, single and multi classes as above; "small" is the
+// segmented sort's kernel for segments that fit one tile.
+#ifndef MGPU_SORT_KEYS_BALLOT_BITS
+#define MGPU_SORT_KEYS_BALLOT_BITS 5
+#endif
+#ifndef MGPU_SORT_SINGLE_BALLOT_BITS
+#define MGPU_SORT_SINGLE_BALLOT_BITS 5
+#endif
+// The single class on sortArray calls of at least LARGE_ELEMENTS keys (the
+// scatter then spans a large array; measured crossover between 32M and 48M).
+#ifndef MGPU_SORT_SINGLE_LARGE_BALLOT_BITS
+#define MGPU_SORT_SINGLE_LARGE_BALLOT_BITS 4
+#endif
+#ifndef MGPU_SORT_SINGLE_LARGE_ELEMENTS
+#define MGPU_SORT_SINGLE_LARGE_ELEMENTS 41943040
+#endif
+#ifndef MGPU_SORT_MULTI_BALLOT_BITS
+#define MGPU_SORT_MULTI_BALLOT_BITS 8
+#endif
+#ifndef MGPU_SORT_SMALL_BALLOT_BITS
+#define MGPU_SORT_SMALL_BALLOT_BITS 5
 #endif
 // Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
 #ifndef MGPU_SORT_MAX_DIGIT_BITS

@@ -51,3 +51,24 @@ def test_every_candidate_fits_shared_memory():
                 words = tile * (2 + (0 if cls == "keys" else 1))
             words += nw * 256 + 4 * 256 + 32 + 16
             assert words * 4 <= 227 * 1024, (cls, threads, items)
+
+
+def test_write_keeps_the_table_of_classes_not_measured(tmp_path):
+    header = tmp_path / "tile_config.h"
+    shutil.copy(autotune.CONFIG_H, header)
+    original = header.read_text()
+    assert "//   keys: chosen " in original
+    keys_block = [l for l in original.splitlines() if l.startswith("//   keys: chosen ")]
+    results = {"small_ballot": {"8": {"w": 1.1}, "5": {"w": 1.0}}}
+    rpath = tmp_path / "r.json"
+    rpath.write_text(json.dumps(results))
+    assert autotune.main(["write", str(rpath), "--header", str(header)]) == 0
+    text = header.read_text()
+    assert keys_block[0] in text                      # kept
+    assert "//   small_ballot: chosen 5" in text       # replaced or added
+    assert text.count("//   small_ballot: chosen") == 1
+    assert "#define MGPU_SORT_SMALL_BALLOT_BITS 5" in text
+    # Classes stay in the autotuner's order.
+    order = [c for c in autotune.CLASSES if f"//   {c}: chosen" in text]
+    pos = [text.index(f"//   {c}: chosen") for c in order]
+    assert pos == sorted(pos)

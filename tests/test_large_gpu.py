@@ -66,3 +66,31 @@ def test_maximum_size_sort(engine, n, value_count, first, end):
     check(d, tensors, src, first, end, torch)
     del tensors, src
     torch.cuda.empty_cache()
+
+
+def _tile_config(name):
+    import os
+    import re
+    path = os.path.join(os.path.dirname(__file__), "..", "mgpu_old_b200", "csrc", "tile_config.h")
+    with open(path) as f:
+        return int(re.search(rf"#define {name} (\d+)", f.read()).group(1))
+
+
+LARGE = _tile_config("MGPU_SORT_SINGLE_LARGE_ELEMENTS")
+
+
+@pytest.mark.parametrize("n", [LARGE - 1, LARGE, LARGE + 7681])
+@pytest.mark.parametrize("value_count,first,end", [(-1, 0, 32), (1, 0, 32), (1, 3, 20)])
+def test_single_class_size_dispatch(engine, n, value_count, first, end):
+    """sortArray with indices or one value array switches ranking kernels at
+    MGPU_SORT_SINGLE_LARGE_ELEMENTS keys; both sides of the switch give the
+    stable sort (exact)."""
+    import torch
+    d, tensors, src = device_data(n, value_count, first, end, torch)
+    torch.cuda.synchronize()
+    assert engine.sort_array(d) == 0
+    assert engine.synchronize() == 0
+    torch.cuda.synchronize()
+    check(d, tensors, src, first, end, torch)
+    del tensors, src
+    torch.cuda.empty_cache()
