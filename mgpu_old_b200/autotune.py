@@ -9,7 +9,8 @@ A candidate is one assignment of tile_config.h's values for one class:
 six value arrays), "digits" (the widest digit of sortArray's pass plan), or
 "<class>_ballot" (how many digit bits the warp ranking of that class resolves
 by ballots, the rest by match.any; "small" is the segmented sort's kernel for
-segments that fit one tile). Each
+segments that fit one tile) or "<class>_batch" (how many items of a thread the
+ranking matches before it updates their digit counters). Each
 candidate is a separate build of the library (build_variant, under
 _build/tune/), because tile shapes are compile-time constants of the
 kernels. The build step runs anywhere nvcc does; the measure step loads each
@@ -81,6 +82,28 @@ CLASSES = {
         "keys": ("MGPU_SORT_MULTI_BALLOT_BITS",),
         "candidates": [(8,), (5,), (4,)],
         "workloads": [("multi6_17bit", 1 << 24), ("multi3_u32", 1 << 24)],
+    },
+    # Items per thread whose peers are found before the counter updates.
+    "keys_batch": {
+        "keys": ("MGPU_SORT_KEYS_RANK_BATCH",),
+        "candidates": [(1,), (4,), (5,), (10,), (20,)],
+        "workloads": [("keys_u32", 1 << 24), ("keys_u32", 1 << 26)],
+    },
+    "single_batch": {
+        "keys": ("MGPU_SORT_SINGLE_RANK_BATCH",),
+        "candidates": [(1,), (4,), (5,), (10,), (20,)],
+        "workloads": [("pairs_and24", 1 << 25), ("pairs_u32", 1 << 26), ("index_u32", 1 << 24),
+                      ("segments_lognormal", 10_000)],
+    },
+    "multi_batch": {
+        "keys": ("MGPU_SORT_MULTI_RANK_BATCH",),
+        "candidates": [(1,), (2,), (4,), (8,)],
+        "workloads": [("multi6_17bit", 1 << 24), ("multi3_u32", 1 << 24)],
+    },
+    "small_batch": {
+        "keys": ("MGPU_SORT_SMALL_RANK_BATCH",),
+        "candidates": [(1,), (2,), (4,), (8,), (16,)],
+        "workloads": [("segments_small", 50_000)],
     },
     "small_ballot": {
         "keys": ("MGPU_SORT_SMALL_BALLOT_BITS",),

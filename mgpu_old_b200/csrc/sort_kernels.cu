@@ -397,6 +397,9 @@ template<int VM> struct SortConfig {
 	static constexpr int kBallotBitsLarge = VM >= 2 ? MGPU_SORT_MULTI_BALLOT_BITS
 		: VM == 0 ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_LARGE_BALLOT_BITS;
 	static constexpr int kLargeElements = MGPU_SORT_SINGLE_LARGE_ELEMENTS;
+	// Items of a thread whose peers are found before their counter updates.
+	static constexpr int kRankBatch = VM >= 2 ? MGPU_SORT_MULTI_RANK_BATCH
+		: VM == 0 ? MGPU_SORT_KEYS_RANK_BATCH : MGPU_SORT_SINGLE_RANK_BATCH;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
@@ -465,13 +468,12 @@ __device__ __forceinline__ unsigned match_digit8(unsigned d,
 	}
 }
 
-// Stable warp rank of one item: the group of peers starts at the warp's
-// running count of the digit, which the highest peer then advances by the
-// group's size. Returns (digit << 16) | rank within the warp.
-template<int BB>
-__device__ __forceinline__ unsigned rank_item(unsigned d, unsigned* warpHist,
-	int lane, unsigned ltMask, const unsigned (&nClear)[4]) {
-	const unsigned peers = match_digit8<BB>(d, nClear);
+// Stable warp rank of one item with digit d and peers (match_digit8): the
+// group of peers starts at the warp's running count of the digit, which the
+// highest peer then advances by the group's size. Returns
+// (digit << 16) | rank within the warp.
+__device__ __forceinline__ unsigned count_item(unsigned d, unsigned peers,
+	unsigned* warpHist, int lane, unsigned ltMask) {
 	// Every peer reads the count; the highest peer then adds the group.
 	const unsigned base = warpHist[d];
 	__syncwarp();
@@ -504,16 +506,29 @@ template<bool BYTE> struct DigitOf {
 // tile element w*32*IPT + i*32 + l, so (item, lane) order is input order per
 // warp). In a partial tile the elements past `count` get digit 255: they
 // rank after every real key and are never stored.
-template<int IPT, bool FULL, bool BYTE, int BB>
+// Items are taken CH at a time: the peers of all CH are found first (the
+// match steps of different items are independent), then the CH counter
+// updates run in item order.
+template<int IPT, bool FULL, bool BYTE, int BB, int CH>
 __device__ __forceinline__ void rank_tile(const unsigned* sKeys, unsigned* myHist,
 	int warpBase, int lane, int count, const DigitOf<BYTE>& digit, unsigned ltMask,
 	const unsigned (&nClear)[4], unsigned (&rank)[IPT]) {
 #pragma unroll
-	for(int i = 0; i < IPT; ++i) {
-		const int idx = warpBase + i * 32 + lane;
-		unsigned d = digit(sKeys[idx]);
-		if(!FULL && idx >= count) d = kDigitBins - 1;
-		rank[i] = rank_item<BB>(d, myHist, lane, ltMask, nClear);
+	for(int c = 0; c < IPT; c += CH) {
+		unsigned d[CH], peers[CH];
+#pragma unroll
+		for(int j = 0; j < CH; ++j) {
+			if(c + j < IPT) {
+				const int idx = warpBase + (c + j) * 32 + lane;
+				d[j] = digit(sKeys[idx]);
+				if(!FULL && idx >= count) d[j] = kDigitBins - 1;
+				peers[j] = match_digit8<BB>(d[j], nClear);
+			}
+		}
+#pragma unroll
+		for(int j = 0; j < CH; ++j) {
+			if(c + j < IPT) rank[c + j] = count_item(d[j], peers[j], myHist, lane, ltMask);
+		}
 	}
 }
 
@@ -718,7 +733,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 			if(!mbar_wait_bounded(&sBar[slot], (phase >> slot) & 1u))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 			phase ^= 1u << slot;
-			rank_tile<IPT, true, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			// Plain loads (a partial tile, or data that is not 16-byte
@@ -729,7 +744,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 					sVals[i] = i < count ? a.buf.valsIn[0][tileStart + i] : 0u;
 			}
 			__syncthreads();
-			rank_tile<IPT, false, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -888,13 +903,13 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 		unsigned rank[IPT];
 		if(bulk) {
 			wait_bar(0);
-			rank_tile<IPT, true, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			for(int i = tid; i < TILE; i += NT)
 				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
 			__syncthreads();
-			rank_tile<IPT, false, BYTE, BB>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -1330,6 +1345,7 @@ seg_sort_kernel(const SegSortArgs a) {
 // the final positions (index mode writes the positions).
 constexpr int kSmallThreads = 256;
 constexpr int kSmallBallotBits = MGPU_SORT_SMALL_BALLOT_BITS;
+constexpr int kSmallRankBatch = MGPU_SORT_SMALL_RANK_BATCH;
 
 struct SmallSortArgs {
 	PassBuffers buf;                // in: [0] arrays; out: the result arrays
@@ -1370,7 +1386,8 @@ __device__ __forceinline__ void small_sort_segment(const SmallSortArgs& a, int b
 	for(int p = 0; p < a.plan.numPasses; ++p) {
 		const DigitOf<false> digit(a.plan.shift[p], a.plan.width[p]);
 		unsigned rank[IPT];
-		rank_tile<IPT, false, false, kSmallBallotBits>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
+		rank_tile<IPT, false, false, kSmallBallotBits,
+			(IPT < kSmallRankBatch ? IPT : kSmallRankBatch)>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
 			lane, len, digit, ltMask, nClear, rank);
 		__syncthreads();
 		unsigned c[NW];

@@ -12,7 +12,9 @@
 //  * <class>_ballot: digit bits the warp ranking of the class resolves by
 //    ballots (match_digit8); single_large_ballot applies to sortArray calls
 //    of at least MGPU_SORT_SINGLE_LARGE_ELEMENTS keys, small_ballot to the
-//    segmented sort's kernel for segments that fit one tile.
+//    segmented sort's kernel for segments that fit one tile;
+//  * <class>_batch: items per thread whose peers are found before their
+//    digit counters are updated (rank_tile).
 // Measured by the autotuner (median ms per sort; score = geometric
 // mean of time / best time over the class's workloads):
 //   keys: chosen 256x20x3
@@ -38,25 +40,48 @@
 //              7  score 1.230  keys_u32_16777216 0.481, pairs_and24_33554432 0.842
 //              6  score 1.333  keys_u32_16777216 0.565, pairs_and24_33554432 0.842
 //   keys_ballot: chosen 5
-//              5  score 1.000  keys_u32_16777216 0.367, keys_u32_67108864 1.247
-//              4  score 1.097  keys_u32_16777216 0.401, keys_u32_67108864 1.370
-//              8  score 1.121  keys_u32_16777216 0.410, keys_u32_67108864 1.403
+//              5  score 1.000  keys_u32_16777216 0.342, keys_u32_67108864 1.165
+//              4  score 1.136  keys_u32_16777216 0.397, keys_u32_67108864 1.294
+//              8  score 1.160  keys_u32_16777216 0.395, keys_u32_67108864 1.358
 //   single_ballot: chosen 5
-//              5  score 1.000  index_u32_16777216 0.463, pairs_and24_33554432 0.623, pairs_u32_16777216 0.469, segments_lognormal_10000 3.916
-//              4  score 1.049  index_u32_16777216 0.496, pairs_and24_33554432 0.625, pairs_u32_16777216 0.498, segments_lognormal_10000 4.166
-//              8  score 1.068  index_u32_16777216 0.496, pairs_and24_33554432 0.668, pairs_u32_16777216 0.500, segments_lognormal_10000 4.159
+//              5  score 1.000  index_u32_16777216 0.457, pairs_and24_33554432 0.602, pairs_u32_16777216 0.461, segments_lognormal_10000 3.809
+//              4  score 1.060  index_u32_16777216 0.487, pairs_and24_33554432 0.614, pairs_u32_16777216 0.492, segments_lognormal_10000 4.132
+//              8  score 1.084  index_u32_16777216 0.494, pairs_and24_33554432 0.664, pairs_u32_16777216 0.494, segments_lognormal_10000 4.120
 //   single_large_ballot: chosen 4
-//              4  score 1.000  index_u32_67108864 1.697, pairs_u32_100663296 2.485, pairs_u32_67108864 1.710
-//              8  score 1.007  index_u32_67108864 1.700, pairs_u32_100663296 2.522, pairs_u32_67108864 1.716
-//              5  score 1.036  index_u32_67108864 1.743, pairs_u32_100663296 2.614, pairs_u32_67108864 1.759
+//              4  score 1.000  index_u32_67108864 1.669, pairs_u32_100663296 2.460, pairs_u32_67108864 1.679
+//              8  score 1.016  index_u32_67108864 1.696, pairs_u32_100663296 2.497, pairs_u32_67108864 1.710
+//              5  score 1.045  index_u32_67108864 1.739, pairs_u32_100663296 2.587, pairs_u32_67108864 1.751
 //   multi_ballot: chosen 8
-//              8  score 1.001  multi3_u32_16777216 0.885, multi6_17bit_16777216 1.210
-//              5  score 1.005  multi3_u32_16777216 0.891, multi6_17bit_16777216 1.210
-//              4  score 1.006  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.225
+//              8  score 1.002  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.212
+//              5  score 1.002  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.213
+//              4  score 1.008  multi3_u32_16777216 0.879, multi6_17bit_16777216 1.231
+//   keys_batch: chosen 20
+//             20  score 1.000  keys_u32_16777216 0.344, keys_u32_67108864 1.169
+//              5  score 1.021  keys_u32_16777216 0.352, keys_u32_67108864 1.190
+//              4  score 1.023  keys_u32_16777216 0.352, keys_u32_67108864 1.196
+//             10  score 1.024  keys_u32_16777216 0.352, keys_u32_67108864 1.198
+//              1  score 1.068  keys_u32_16777216 0.367, keys_u32_67108864 1.251
+//   single_batch: chosen 10
+//             10  score 1.000  index_u32_16777216 0.459, pairs_and24_33554432 0.602, pairs_u32_67108864 1.681, segments_lognormal_10000 3.827
+//              5  score 1.006  index_u32_16777216 0.461, pairs_and24_33554432 0.605, pairs_u32_67108864 1.700, segments_lognormal_10000 3.832
+//              4  score 1.006  index_u32_16777216 0.461, pairs_and24_33554432 0.606, pairs_u32_67108864 1.702, segments_lognormal_10000 3.827
+//              1  score 1.024  index_u32_16777216 0.467, pairs_and24_33554432 0.625, pairs_u32_67108864 1.708, segments_lognormal_10000 3.923
+//             20  score 1.071  index_u32_16777216 0.490, pairs_and24_33554432 0.666, pairs_u32_67108864 1.859, segments_lognormal_10000 3.852
+//   multi_batch: chosen 8
+//              8  score 1.000  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.206
+//              4  score 1.001  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.208
+//              2  score 1.004  multi3_u32_16777216 0.889, multi6_17bit_16777216 1.208
+//              1  score 1.008  multi3_u32_16777216 0.893, multi6_17bit_16777216 1.210
+//   small_batch: chosen 8
+//              8  score 1.000  segments_small_50000 0.993
+//             16  score 1.000  segments_small_50000 0.993
+//              4  score 1.002  segments_small_50000 0.995
+//              2  score 1.014  segments_small_50000 1.008
+//              1  score 1.039  segments_small_50000 1.032
 //   small_ballot: chosen 5
-//              5  score 1.000  segments_small_50000 1.026
-//              4  score 1.018  segments_small_50000 1.045
-//              8  score 1.054  segments_small_50000 1.081
+//              5  score 1.000  segments_small_50000 0.987
+//              4  score 1.029  segments_small_50000 1.016
+//              8  score 1.079  segments_small_50000 1.065
 #pragma once
 
 #ifndef MGPU_SORT_KEYS_THREADS
@@ -108,6 +133,20 @@
 #endif
 #ifndef MGPU_SORT_SMALL_BALLOT_BITS
 #define MGPU_SORT_SMALL_BALLOT_BITS 5
+#endif
+// Items of a thread whose peers the warp ranking finds before it updates
+// their digit counters (1: one item at a time), per class.
+#ifndef MGPU_SORT_KEYS_RANK_BATCH
+#define MGPU_SORT_KEYS_RANK_BATCH 20
+#endif
+#ifndef MGPU_SORT_SINGLE_RANK_BATCH
+#define MGPU_SORT_SINGLE_RANK_BATCH 10
+#endif
+#ifndef MGPU_SORT_MULTI_RANK_BATCH
+#define MGPU_SORT_MULTI_RANK_BATCH 8
+#endif
+#ifndef MGPU_SORT_SMALL_RANK_BATCH
+#define MGPU_SORT_SMALL_RANK_BATCH 8
 #endif
 // Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
 #ifndef MGPU_SORT_MAX_DIGIT_BITS
