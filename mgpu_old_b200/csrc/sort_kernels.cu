@@ -45,19 +45,26 @@ __device__ __forceinline__ void allow_successor() {
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// carveout >= 0 also sets this launch's preferred shared-memory carveout
+// (percent of the L1/shared capacity).
 template<typename Arg>
 static cudaError_t launch_dependent(void (*kernel)(Arg), int grid, int block,
-	size_t smem, cudaStream_t stream, const Arg& arg) {
+	size_t smem, cudaStream_t stream, const Arg& arg, int carveout = -1) {
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3(grid);
 	cfg.blockDim = dim3(block);
 	cfg.dynamicSmemBytes = smem;
 	cfg.stream = stream;
-	cudaLaunchAttribute attr[1];
+	cudaLaunchAttribute attr[2];
 	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
 	attr[0].val.programmaticStreamSerializationAllowed = 1;
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
+	if(carveout >= 0) {
+		attr[1].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+		attr[1].val.sharedMemCarveout = (unsigned)carveout;
+		cfg.numAttrs = 2;
+	}
 	return cudaLaunchKernelEx(&cfg, kernel, arg);
 }
 
@@ -1525,6 +1532,19 @@ static cudaError_t set_sort_attributes() {
 cudaError_t configure_kernels() {
 	cudaError_t e = cudaSuccess;
 	cudaError_t r;
+#if MGPU_SORT_SEG_SHARED_CARVEOUT
+	{
+		const cudaFuncAttribute c = cudaFuncAttributePreferredSharedMemoryCarveout;
+		const int v = (int)cudaSharedmemCarveoutMaxShared;
+		if((r = cudaFuncSetAttribute(seg_plan_kernel, c, v)) != cudaSuccess) e = r;
+		if((r = cudaFuncSetAttribute(seg_count_kernel, c, v)) != cudaSuccess) e = r;
+		if((r = cudaFuncSetAttribute(seg_scan_kernel, c, v)) != cudaSuccess) e = r;
+		if((r = cudaFuncSetAttribute(small_sort_kernel<kSegTinyMax / kSmallThreads>, c, v))
+			!= cudaSuccess) e = r;
+		if((r = cudaFuncSetAttribute(small_sort_kernel<kSegSmallMax / kSmallThreads>, c, v))
+			!= cudaSuccess) e = r;
+	}
+#endif
 	if((r = set_sort_attributes<-1>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<0>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<1>()) != cudaSuccess) e = r;
@@ -1621,8 +1641,14 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
 	c.split = split;
 	c.rangeCounts = rangeCounts;
+	// Small sorts: count and scan take the sort kernel's carveout, so that
+	// no SM has to change its L1/shared split (which it can only do when
+	// idle) between the kernels of a pass. Larger sorts leave the count
+	// kernel its default, larger L1.
+	const int carveout = (long long)n <= MGPU_SORT_CARVEOUT_MAX_ELEMENTS
+		? (int)cudaSharedmemCarveoutMaxShared : -1;
 	cudaError_t e = launch_dependent(count_kernel, split.numRanges, kCountThreads, 0,
-		stream, c);
+		stream, c, carveout);
 	if(e != cudaSuccess) return e;
 
 	ScanArgs s;
@@ -1631,7 +1657,7 @@ cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	s.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
 	s.numRanges = split.numRanges;
 	return launch_dependent(scan_kernel, kDigitBins, (split.numRanges + 31) / 32 * 32, 0,
-		stream, s);
+		stream, s, carveout);
 }
 
 template<int VM, int BB>

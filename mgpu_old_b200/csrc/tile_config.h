@@ -148,6 +148,15 @@
 #ifndef MGPU_SORT_SMALL_RANK_BATCH
 #define MGPU_SORT_SMALL_RANK_BATCH 8
 #endif
+// sortArray calls of at most CARVEOUT_MAX_ELEMENTS keys run the count and
+// scan kernels with the sort kernel's (largest) shared-memory carveout.
+#ifndef MGPU_SORT_CARVEOUT_MAX_ELEMENTS
+#define MGPU_SORT_CARVEOUT_MAX_ELEMENTS 1048576
+#endif
+// 1: the segmented sort's kernels all take the largest carveout.
+#ifndef MGPU_SORT_SEG_SHARED_CARVEOUT
+#define MGPU_SORT_SEG_SHARED_CARVEOUT 0
+#endif
 // Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
 #ifndef MGPU_SORT_MAX_DIGIT_BITS
 #define MGPU_SORT_MAX_DIGIT_BITS 8
