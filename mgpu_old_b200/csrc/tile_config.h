@@ -17,24 +17,24 @@
 //    digit counters are updated (rank_tile).
 // Measured by the autotuner (median ms per sort; score = geometric
 // mean of time / best time over the class's workloads):
-//   keys: chosen 256x20x3
-//       256x20x3  score 1.032  keys_u32_1048576 0.076, keys_u32_16777216 0.403, keys_u32_67108864 1.401
-//       512x14x2  score 1.043  keys_u32_1048576 0.080, keys_u32_16777216 0.385, keys_u32_67108864 1.438
-//       384x20x2  score 1.050  keys_u32_1048576 0.082, keys_u32_16777216 0.397, keys_u32_67108864 1.387
-//       512x16x2  score 1.053  keys_u32_1048576 0.084, keys_u32_16777216 0.381, keys_u32_67108864 1.423
-//       384x24x2  score 1.059  keys_u32_1048576 0.090, keys_u32_16777216 0.379, keys_u32_67108864 1.358
+//   keys: chosen 512x14x2
+//       512x14x2  score 1.030  keys_u32_1048576 0.059, keys_u32_16777216 0.336, keys_u32_67108864 1.243
+//       384x20x2  score 1.036  keys_u32_1048576 0.061, keys_u32_16777216 0.342, keys_u32_67108864 1.202
+//       384x24x2  score 1.049  keys_u32_1048576 0.068, keys_u32_16777216 0.328, keys_u32_67108864 1.184
+//       256x20x3  score 1.059  keys_u32_1048576 0.068, keys_u32_16777216 0.342, keys_u32_67108864 1.167
+//       512x16x2  score 1.077  keys_u32_1048576 0.070, keys_u32_16777216 0.332, keys_u32_67108864 1.229
 //   single: chosen 384x20x2
-//       384x20x2  score 1.000  index_u32_16777216 0.496, pairs_and24_33554432 0.676, pairs_u32_67108864 1.729
-//       512x14x2  score 1.021  index_u32_16777216 0.500, pairs_and24_33554432 0.696, pairs_u32_67108864 1.772
-//       256x24x2  score 1.028  index_u32_16777216 0.498, pairs_and24_33554432 0.686, pairs_u32_67108864 1.839
-//       384x16x2  score 1.029  index_u32_16777216 0.500, pairs_and24_33554432 0.690, pairs_u32_67108864 1.827
-//       768x10x1  score 1.108  index_u32_16777216 0.526, pairs_and24_33554432 0.764, pairs_u32_67108864 1.957
-//       256x20x3  score 1.145  index_u32_16777216 0.571, pairs_and24_33554432 0.693, pairs_u32_67108864 2.193
+//       384x20x2  score 1.000  index_u32_16777216 0.455, pairs_and24_33554432 0.600, pairs_u32_67108864 1.686
+//       512x14x2  score 1.022  index_u32_16777216 0.461, pairs_and24_33554432 0.621, pairs_u32_67108864 1.714
+//       256x24x2  score 1.064  index_u32_16777216 0.485, pairs_and24_33554432 0.604, pairs_u32_67108864 1.888
+//       384x16x2  score 1.071  index_u32_16777216 0.483, pairs_and24_33554432 0.616, pairs_u32_67108864 1.894
+//       768x10x1  score 1.160  index_u32_16777216 0.489, pairs_and24_33554432 0.692, pairs_u32_67108864 2.119
+//       256x20x3  score 1.240  index_u32_16777216 0.567, pairs_and24_33554432 0.707, pairs_u32_67108864 2.186
 //   multi: chosen 768x8x1
-//        768x8x1  score 1.002  multi3_u32_16777216 0.879, multi6_17bit_16777216 1.217
-//       512x12x1  score 1.008  multi3_u32_16777216 0.874, multi6_17bit_16777216 1.235
-//       384x16x1  score 1.022  multi3_u32_16777216 0.881, multi6_17bit_16777216 1.262
-//       576x10x1  score 1.033  multi3_u32_16777216 0.899, multi6_17bit_16777216 1.264
+//        768x8x1  score 1.000  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.202
+//       512x12x1  score 1.007  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.219
+//       384x16x1  score 1.023  multi3_u32_16777216 0.893, multi6_17bit_16777216 1.243
+//       576x10x1  score 1.027  multi3_u32_16777216 0.901, multi6_17bit_16777216 1.241
 //   digits: chosen 8
 //              8  score 1.000  keys_u32_16777216 0.397, pairs_and24_33554432 0.674
 //              7  score 1.230  keys_u32_16777216 0.481, pairs_and24_33554432 0.842
@@ -85,13 +85,13 @@
 #pragma once
 
 #ifndef MGPU_SORT_KEYS_THREADS
-#define MGPU_SORT_KEYS_THREADS 256
+#define MGPU_SORT_KEYS_THREADS 512
 #endif
 #ifndef MGPU_SORT_KEYS_ITEMS
-#define MGPU_SORT_KEYS_ITEMS 20
+#define MGPU_SORT_KEYS_ITEMS 14
 #endif
 #ifndef MGPU_SORT_KEYS_MIN_BLOCKS
-#define MGPU_SORT_KEYS_MIN_BLOCKS 3
+#define MGPU_SORT_KEYS_MIN_BLOCKS 2
 #endif
 #ifndef MGPU_SORT_SINGLE_THREADS
 #define MGPU_SORT_SINGLE_THREADS 384

@@ -40,8 +40,8 @@ def test_golden_fixtures(engine, path):
 
 
 # Around the tile sizes of the sort kernel with the shipped tile shapes
-# (5120 keys only, 7680 indices or one value array, 6144 several value
-# arrays), two tiles, and of other shapes the autotuner may pick.
+# (7168 keys only, 7680 indices or one value array, 6144 several value
+# arrays), two tiles, and of other shapes the autotuner may pick (5120).
 SIZES = [1, 2, 31, 255, 4095, 4097, 5119, 5120, 5121, 6143, 6144, 6145, 7167, 7168,
          7169, 7679, 7680, 7681, 10241, 12289, 15361, 100003]
 
