@@ -47,6 +47,11 @@ FALLBACK_HBM_GBS = 6650.0
 CPU_SAMPLE = 1 << 22
 
 
+# Batches in flight in the end-to-end measurement (one engine, stream and
+# set of device buffers each).
+E2E_LANES = 3
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -948,15 +953,15 @@ def main():
 
     # End to end through the C ABI with pinned host buffers: every step
     # copies its inputs in, sorts (sortArrayAsync) and copies the sorted keys
-    # and values out. Two batches are in flight, each with its own engine,
-    # stream and device buffers, so one batch's copies overlap the other's
-    # sort and copies in the opposite direction, as a caller streaming
-    # batches through the library would run it. CUDA events on the two
-    # streams bracket all steps.
-    sorter2 = GpuSorter(case, device)
-    engine2 = api.MgpuSort()
-    lanes = [(sorter, engine, torch.cuda.Stream(device)),
-             (sorter2, engine2, torch.cuda.Stream(device))]
+    # and values out. E2E_LANES batches are in flight, each with its own
+    # engine, stream and device buffers, as a caller streaming batches
+    # through the library would run it: one batch's copies in overlap
+    # another's copies out, and with three lanes a batch's copy in never
+    # waits for the copy out of the batch before it on the same lane. CUDA
+    # events on the streams bracket all steps.
+    extra = [(GpuSorter(case, device), api.MgpuSort()) for _ in range(E2E_LANES - 1)]
+    lanes = [(sorter, engine, torch.cuda.Stream(device))] + \
+        [(srt, eng, torch.cuda.Stream(device)) for srt, eng in extra]
     pinned_in = [torch.from_numpy(case.keys.view(np.int32)).pin_memory()] + \
         [torch.from_numpy(v.view(np.int32)).pin_memory() for v in case.values]
     pinned_out = [[torch.empty(case.n, dtype=torch.int32).pin_memory()
@@ -965,9 +970,9 @@ def main():
     d2h = 4 * case.n * len(pinned_out[0])
 
     def e2e_step(j):
-        srt, eng, st = lanes[j % 2]
+        srt, eng, st = lanes[j % len(lanes)]
         dd = srt.data
-        out = pinned_out[j % 2]
+        out = pinned_out[j % len(lanes)]
         with torch.cuda.stream(st):
             srt.bufs[dd.keys[0]][:case.n].copy_(pinned_in[0], non_blocking=True)
             for i in range(len(case.values)):
@@ -981,36 +986,40 @@ def main():
                 out[1 + i].copy_(srt.bufs[dd.values[i][0]][:case.n], non_blocking=True)
 
     def e2e_run(steps, inflight):
+        """Steps spread over the first `inflight` lanes (1: one batch at a
+        time, each step waiting for the previous one)."""
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e0.record(lanes[0][2])
-        lanes[1][2].wait_event(e0)
+        for _, _, st in lanes[1:inflight]:
+            st.wait_event(e0)
         for j in range(steps):
-            k = j if inflight == 2 else 0
             if inflight == 1 and j:
                 lanes[0][2].synchronize()
-            e2e_step(k)
-        done = torch.cuda.Event()
-        done.record(lanes[1][2])
-        lanes[0][2].wait_event(done)
+            e2e_step(j % inflight)
+        for _, _, st in lanes[1:inflight]:
+            done = torch.cuda.Event()
+            done.record(st)
+            lanes[0][2].wait_event(done)
         e1 = torch.cuda.Event(enable_timing=True)
         e1.record(lanes[0][2])
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    e2e_run(2, 2)   # warm the second engine and the copy paths
+    e2e_run(len(lanes), len(lanes))   # warm every engine and the copy paths
     barrier()
-    e2e_ms = max_over_ranks(e2e_run(args.steps, 2))
+    e2e_ms = max_over_ranks(e2e_run(args.steps, len(lanes)))
     e2e_serial_ms = max_over_ranks(e2e_run(max(2, args.steps // 4), 1))
-    api.check(engine.synchronize())
-    api.check(engine2.synchronize())
-    last = (args.steps - 1) % 2
+    for _, eng, _ in lanes:
+        api.check(eng.synchronize())
+    last = (args.steps - 1) % len(lanes)
     verify(case, pinned_out[last][0].numpy().view(np.uint32),
            [p.numpy().view(np.uint32) for p in pinned_out[last][1:]])
     e2e_value = case.n * world / (e2e_ms / args.steps * 1e-3) / 1e6
     e2e_serial = case.n * world / (e2e_serial_ms / max(2, args.steps // 4) * 1e-3) / 1e6
-    engine2.release()
-    del sorter2
+    for _, eng in extra:
+        eng.release()
+    del extra
 
     # Roofline of the sort kernel of a pass.
     peak, peak_src = hbm_peak()
@@ -1040,7 +1049,7 @@ def main():
             "data": "synthetic (seeded numpy MT19937)",
             "config": workload_config(case, args),
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "batches_in_flight": 2,
+                    "d2h_bytes_per_step": d2h, "batches_in_flight": E2E_LANES,
                     "one_batch_at_a_time": round(e2e_serial, 1)},
             # per pass: count + scan kernels (one timed "upsweep" entry) and
             # the sort kernel
