@@ -450,10 +450,11 @@ template<int VM> struct SortLayout {
 //   BB = 8: four more ballots build a second 16-entry table for the high
 //           nibble; peers = low entry & high entry (two shuffles);
 //   BB = 5: a fifth ballot widens the table to 32 entries (bit 4 of the
-//           lane), and match.any on the top three bits gives the rest;
+//           lane: blocks are one-dimensional, so threadIdx.x & 16), and
+//           match.any on the top three bits gives the rest;
 //   BB = 4: match.any on the high nibble.
-// All three return the same set; which is fastest depends on the tile shape
-// and is a choice of the autotuner.
+// All three return the same set; which is fastest depends on the value mode
+// and the array size and is a choice of the autotuner.
 template<int BB>
 __device__ __forceinline__ unsigned match_digit8(unsigned d,
 	const unsigned (&nClear)[4]) {
@@ -684,6 +685,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 	using L = SortLayout<VM>;
 	constexpr int NT = L::NT;
 	constexpr int IPT = L::IPT;
+	constexpr int CH = SortConfig<VM>::kRankBatch;
 	constexpr int TILE = L::TILE;
 	constexpr int NW = L::NW;
 	constexpr int NV = L::NV;
@@ -740,7 +742,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 			if(!mbar_wait_bounded(&sBar[slot], (phase >> slot) & 1u))
 				report_error(a.devError, a.hostError, kErrBarrierTimeout);
 			phase ^= 1u << slot;
-			rank_tile<IPT, true, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB, CH>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			// Plain loads (a partial tile, or data that is not 16-byte
@@ -751,7 +753,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 					sVals[i] = i < count ? a.buf.valsIn[0][tileStart + i] : 0u;
 			}
 			__syncthreads();
-			rank_tile<IPT, false, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB, CH>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
@@ -857,6 +859,7 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 	using L = SortLayout<VM>;
 	constexpr int NT = L::NT;
 	constexpr int IPT = L::IPT;
+	constexpr int CH = SortConfig<VM>::kRankBatch;
 	constexpr int TILE = L::TILE;
 	constexpr int NV = L::NV;
 	constexpr unsigned kTileBytes = TILE * 4;
@@ -910,13 +913,13 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 		unsigned rank[IPT];
 		if(bulk) {
 			wait_bar(0);
-			rank_tile<IPT, true, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, true, BYTE, BB, CH>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		} else {
 			for(int i = tid; i < TILE; i += NT)
 				sKeys[i] = i < count ? a.buf.keysIn[tileStart + i] : 0xffffffffu;
 			__syncthreads();
-			rank_tile<IPT, false, BYTE, BB, SortConfig<VM>::kRankBatch>(sKeys, myHist, warpBase, lane, count, digit,
+			rank_tile<IPT, false, BYTE, BB, CH>(sKeys, myHist, warpBase, lane, count, digit,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
