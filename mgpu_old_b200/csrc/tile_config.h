@@ -40,9 +40,9 @@
 //              7  score 1.230  keys_u32_16777216 0.481, pairs_and24_33554432 0.842
 //              6  score 1.333  keys_u32_16777216 0.565, pairs_and24_33554432 0.842
 //   keys_ballot: chosen 5
-//              5  score 1.000  keys_u32_16777216 0.342, keys_u32_67108864 1.165
-//              4  score 1.136  keys_u32_16777216 0.397, keys_u32_67108864 1.294
-//              8  score 1.160  keys_u32_16777216 0.395, keys_u32_67108864 1.358
+//              5  score 1.000  keys_u32_16777216 0.336, keys_u32_67108864 1.243
+//              8  score 1.141  keys_u32_16777216 0.381, keys_u32_67108864 1.427
+//              4  score 1.150  keys_u32_16777216 0.387, keys_u32_67108864 1.425
 //   single_ballot: chosen 5
 //              5  score 1.000  index_u32_16777216 0.457, pairs_and24_33554432 0.602, pairs_u32_16777216 0.461, segments_lognormal_10000 3.809
 //              4  score 1.060  index_u32_16777216 0.487, pairs_and24_33554432 0.614, pairs_u32_16777216 0.492, segments_lognormal_10000 4.132
@@ -55,12 +55,12 @@
 //              8  score 1.002  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.212
 //              5  score 1.002  multi3_u32_16777216 0.883, multi6_17bit_16777216 1.213
 //              4  score 1.008  multi3_u32_16777216 0.879, multi6_17bit_16777216 1.231
-//   keys_batch: chosen 20
-//             20  score 1.000  keys_u32_16777216 0.344, keys_u32_67108864 1.169
-//              5  score 1.021  keys_u32_16777216 0.352, keys_u32_67108864 1.190
-//              4  score 1.023  keys_u32_16777216 0.352, keys_u32_67108864 1.196
-//             10  score 1.024  keys_u32_16777216 0.352, keys_u32_67108864 1.198
-//              1  score 1.068  keys_u32_16777216 0.367, keys_u32_67108864 1.251
+//   keys_batch: chosen 5
+//              5  score 1.000  keys_u32_16777216 0.336, keys_u32_67108864 1.237
+//             20  score 1.002  keys_u32_16777216 0.336, keys_u32_67108864 1.243
+//              4  score 1.011  keys_u32_16777216 0.338, keys_u32_67108864 1.255
+//              1  score 1.019  keys_u32_16777216 0.342, keys_u32_67108864 1.262
+//             10  score 1.020  keys_u32_16777216 0.342, keys_u32_67108864 1.264
 //   single_batch: chosen 10
 //             10  score 1.000  index_u32_16777216 0.459, pairs_and24_33554432 0.602, pairs_u32_67108864 1.681, segments_lognormal_10000 3.827
 //              5  score 1.006  index_u32_16777216 0.461, pairs_and24_33554432 0.605, pairs_u32_67108864 1.700, segments_lognormal_10000 3.832
@@ -137,7 +137,7 @@
 // Items of a thread whose peers the warp ranking finds before it updates
 // their digit counters (1: one item at a time), per class.
 #ifndef MGPU_SORT_KEYS_RANK_BATCH
-#define MGPU_SORT_KEYS_RANK_BATCH 20
+#define MGPU_SORT_KEYS_RANK_BATCH 5
 #endif
 #ifndef MGPU_SORT_SINGLE_RANK_BATCH
 #define MGPU_SORT_SINGLE_RANK_BATCH 10
