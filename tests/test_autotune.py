@@ -72,3 +72,34 @@ def test_write_keeps_the_table_of_classes_not_measured(tmp_path):
     order = [c for c in autotune.CLASSES if f"//   {c}: chosen" in text]
     pos = [text.index(f"//   {c}: chosen") for c in order]
     assert pos == sorted(pos)
+
+
+def test_segmented_check_is_exact():
+    """The autotuner's check of segmented results accepts the stable
+    per-segment sort and rejects a swap of two equal-key positions."""
+    import numpy as np
+    import pytest
+    case = autotune.make_case("segments_small", 200)
+    keys = case.keys.copy()
+    keys[::3] &= np.uint32(0xF)                 # many ties
+    case.keys = keys
+    out_k = np.empty_like(keys)
+    out_v = np.empty_like(keys)
+    for i in range(case.num_segments):
+        a, b = int(case.offsets[i]), int(case.offsets[i + 1])
+        o = np.argsort(keys[a:b], kind="stable")
+        out_k[a:b] = keys[a:b][o]
+        out_v[a:b] = case.values[0][a:b][o]
+    autotune.check_segmented(case, out_k, out_v)
+    # Two adjacent equal keys of one segment with their positions swapped.
+    for i in range(case.num_segments):
+        a, b = int(case.offsets[i]), int(case.offsets[i + 1])
+        eq = np.flatnonzero(out_k[a + 1:b] == out_k[a:b - 1])
+        if eq.size:
+            j = a + int(eq[0])
+            bad = out_v.copy()
+            bad[[j, j + 1]] = bad[[j + 1, j]]
+            with pytest.raises(RuntimeError):
+                autotune.check_segmented(case, out_k, bad)
+            return
+    raise AssertionError("no tie found")
