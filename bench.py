@@ -4,25 +4,26 @@
                     [--impl ours|reference]
 
 A step is one sortArray call over one batch of synthetic input (default:
-33,554,432 uint32 key + value pairs, keys = AND of two uniform draws masked to
-24 bits, value = index, bits [0, 24)). Each timed step starts from freshly
-restored input and a flushed L2 (a 256 MiB write between steps; the restore
-copy and the flush are outside the timed region). `value` is device-resident
-throughput in Mkeys/s over the K timed steps (CUDA events on the sort's
-stream, max over ranks); `e2e` is the same metric through the C ABI with
-pinned host buffers, host->device and device->host copies inside the timed
-region. The roofline entry is the sort kernel of a pass (the dominant kernel),
-whose launches are timed with CUDA events inside the same timed steps
-(sortEnableKernelTiming).
+67,108,864 uint32 key + value pairs, keys uniform over 32 bits, value =
+index, bits [0, 32): the 64M-pair target configuration). Each timed step
+starts from freshly restored input and a flushed L2 (a 256 MiB write between
+steps; the restore copy and the flush are outside the timed region). `value`
+is device-resident throughput in Mkeys/s over the K timed steps (CUDA events
+on the sort's stream, max over ranks); `e2e` is the same metric through the C
+ABI with pinned host buffers, host->device and device->host copies inside the
+timed region. The roofline entry is the sort kernel of a pass (the dominant
+kernel), whose launches are timed with CUDA events inside the same timed
+steps (sortEnableKernelTiming).
 
 Multi-GPU: the sort path does not shard (one global order), so N ranks run N
 independent replicas of the workload ("weak" scaling); the only collectives
 are the barrier and the max-over-ranks of the timings.
 
---impl reference times the reference's CPU sort path on this host: the CPU
-radix sort of sort/src/cpusort/cpusort.cpp:122-186 as restated by the
-oracle (extended to values and bit ranges) on all host threads, over a
-bounded sample of the same workload per step.
+--impl reference times the reference's CPU sort path on this host over the
+whole workload per step: for keys-only uint32 workloads the reference's own
+sort/src/cpusort/cpusort.cpp compiled from its source (oracle/_ref), else the
+oracle's restatement of its algorithm (cpusort.cpp:122-186) extended to value
+arrays, on all host threads. That arm never loads the library.
 """
 from __future__ import annotations
 
@@ -58,7 +59,7 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="pairs_and24_32M",
+    p.add_argument("--workload", default="pairs_u32_64M",
                    choices=sorted(workloads.WORKLOADS) + ["served", "bwt"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--server-slots", type=int, default=4,
@@ -96,8 +97,12 @@ def workload_config(case, args, extra=None):
 
 
 def _plan(case):
-    from mgpu_old_b200 import api
-    return api.plan_passes(case.first_bit, case.end_bit)
+    """sortArray's pass widths over the case's bit range: ceil(bits / 8)
+    passes, widths balanced. Plain Python, so that the CPU arms never load the
+    library."""
+    bits = case.end_bit - case.first_bit
+    p = (bits + 7) // 8
+    return [bits // p + (i < bits % p) for i in range(p)]
 
 
 # ---------------------------------------------------------------------------
@@ -210,42 +215,105 @@ def run_reference_bwt(args):
 
 
 # ---------------------------------------------------------------------------
-# CPU side: the oracle's blocked LSD radix sort (cpusort.cpp:122-186 restated)
+# CPU side. The reference's CPU sort (sort/src/cpusort/cpusort.cpp) sorts keys
+# only: for keys-only workloads its own code, compiled from its source into
+# oracle/_ref, is timed ("reference"); where values ride along, the oracle's
+# LSD restatement of the same algorithm (cpusort.cpp:122-186, extended to
+# value arrays and bit ranges, its per-block phases on all host threads) is
+# timed instead ("port").
 
 
-def cpu_sort_sample(case, sample_n, threads):
-    """Time the oracle's multithreaded LSD sort on the first sample_n elements.
-    Returns seconds of one sort."""
+def _lsd_full(case, threads):
+    """The oracle's LSD sort of the whole workload on `threads` host threads.
+    Returns (seconds, keys, values)."""
+    from oracle import oracle
+    oracle.build(ref=False)
+    t0 = time.perf_counter()
+    keys = case.keys
+    if case.key_type:
+        keys = workloads.key_image(keys, case.key_type)
+    k, v = oracle.sort_lsd(keys, case.values, case.value_count, case.first_bit,
+                           _plan(case), 1 << 15, threads)
+    if case.key_type:
+        k = workloads.key_preimage(k, case.key_type)
+    return time.perf_counter() - t0, k, v
+
+
+def _ref_sort2_usable(case):
+    """The reference's own CPU sort handles this workload: uint32 keys only."""
+    if case.value_count != 0 or case.key_type:
+        return False
+    from oracle import oracle
+    return oracle.ref_lib() is not None
+
+
+def _ref_sort2(case):
+    """The reference's CPU radix sort (cpusort.cpp Sort2Pass, blocked 4-bit
+    passes as its Sort2 makes them, sequential as written) over the case's
+    bit range. Returns (seconds, keys)."""
+    from oracle import oracle
+    ref = oracle.ref_lib()
+    k = np.array(case.keys, dtype=np.uint32, copy=True)
+    t0 = time.perf_counter()
+    bit = case.first_bit
+    while bit < case.end_bit:
+        nb = min(4, case.end_bit - bit)
+        ref.ref_cpusort_sort2pass(oracle._p(k), bit, nb, k.size, 2048)
+        bit += nb
+    return time.perf_counter() - t0, k
+
+
+def _stable_sample(case, sample_n):
+    """std::stable_sort by the bit field (the oracle's stable leg) on one
+    core over the first sample_n elements. Returns seconds."""
     from oracle import oracle
     oracle.build(ref=False)
     keys = np.ascontiguousarray(case.keys[:sample_n])
-    vals = [np.ascontiguousarray(v[:sample_n]) for v in case.values]
-    bits = case.end_bit - case.first_bit
-    p = (bits + 7) // 8
-    widths = [bits // p + (i < bits % p) for i in range(p)]
-    t0 = time.perf_counter()
     if case.key_type:
-        # Signed / float keys: the same transform, sort and inverse on the host.
         keys = workloads.key_image(keys, case.key_type)
-    oracle.sort_lsd(keys, vals, case.value_count, case.first_bit, widths, 1 << 15, threads)
-    if case.key_type:
-        keys = workloads.key_preimage(keys, case.key_type)
+    vals = [np.ascontiguousarray(v[:sample_n]) for v in case.values]
+    t0 = time.perf_counter()
+    oracle.sort_stable(keys, vals, case.value_count, case.first_bit, case.end_bit)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(case, budget_s=10.0):
+def cpu_baseline(case, gpu_keys, gpu_vals, budget_s=20.0):
+    """Times the CPU path on the host cores over the whole workload and, as
+    the checker, compares the GPU result with its output bit for bit (keys
+    and every value array). Also reports std::stable_sort on one core over a
+    bounded sample and, for keys-only workloads, the reference's own Sort2."""
     threads = os.cpu_count() or 1
+    t, k, v = _lsd_full(case, threads)
+    if not np.array_equal(k, gpu_keys):
+        raise AssertionError("GPU keys differ from the oracle")
+    for i, (a, b) in enumerate(zip(gpu_vals, v)):
+        if not np.array_equal(a, b):
+            raise AssertionError(f"GPU value array {i} differs from the oracle")
+    times = [t]
+    t_end = time.perf_counter() + budget_s / 2
+    while time.perf_counter() < t_end and len(times) < 5:
+        times.append(_lsd_full(case, threads)[0])
+    lsd_t = min(times)
+    out = {"value": round(case.n / lsd_t / 1e6, 3), "unit": UNIT, "cores": threads,
+           "kind": "port",
+           "sample": f"the whole workload ({case.n} elements, all value arrays), oracle LSD "
+                     f"radix (cpusort.cpp:122-186 restated, 8-bit passes) on {threads} "
+                     f"threads, best of {len(times)}",
+           "oracle_check": "GPU keys and every value array equal the oracle's, bit for bit"}
     sample_n = min(case.n, CPU_SAMPLE)
-    total_t, total_n = 0.0, 0
-    t_end = time.perf_counter() + budget_s
-    while time.perf_counter() < t_end or total_n == 0:
-        total_t += cpu_sort_sample(case, sample_n, threads)
-        total_n += sample_n
-    return {"value": round(total_n / total_t / 1e6, 3), "unit": UNIT, "cores": threads,
-            "kind": "port",
-            "sample": f"first {sample_n} elements of {case.name}, oracle LSD radix "
-                      f"(cpusort.cpp:122-186 restated) on {threads} threads, "
-                      f"{total_n // sample_n} repetitions"}
+    st = _stable_sample(case, sample_n)
+    out["std_stable_sort"] = {"value": round(sample_n / st / 1e6, 3), "unit": UNIT, "cores": 1,
+                              "sample": f"first {sample_n} elements, std::stable_sort of "
+                                        "positions by the bit field, values gathered"}
+    if _ref_sort2_usable(case):
+        rt, rk = _ref_sort2(case)
+        if not np.array_equal(rk, gpu_keys):
+            raise AssertionError("GPU keys differ from the reference's own CPU sort")
+        out["reference_sort2"] = {"value": round(case.n / rt / 1e6, 3), "unit": UNIT,
+                                  "cores": 1, "kind": "reference",
+                                  "sample": "the whole workload, cpusort.cpp Sort2Pass "
+                                            "4-bit passes built from the reference source"}
+    return out
 
 
 def cpu_baseline_segmented(case, budget_s=10.0):
@@ -346,6 +414,13 @@ def run_reference_served(args):
 
 
 def run_reference(args):
+    """Reference arm: the reference's CPU sort path over the whole workload
+    per step, on this host's cores. Keys-only uint32 workloads run the
+    reference's own cpusort.cpp (Sort2Pass, compiled from its source into
+    oracle/_ref; sequential code, one thread); workloads with value arrays
+    run the oracle's restatement of it extended to values, on all host
+    threads. Warm-up is capped at one step and the timed steps at a time
+    budget, so that the arm ends within a few minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -357,20 +432,40 @@ def run_reference(args):
     if isinstance(case, workloads.SegmentedCase):
         return run_reference_segmented(args, case)
     threads = os.cpu_count() or 1
-    sample_n = min(case.n, CPU_SAMPLE)
-    for _ in range(args.warmup):
-        cpu_sort_sample(case, sample_n, threads)
-    times = [cpu_sort_sample(case, sample_n, threads) for _ in range(args.steps)]
+    if _ref_sort2_usable(case):
+        kind, cores = "reference", 1
+        what = "cpusort.cpp Sort2Pass (blocked 4-bit passes) built from the reference source"
+
+        def step():
+            return _ref_sort2(case)[0]
+    else:
+        kind, cores = "port", threads
+        what = (f"oracle LSD radix (cpusort.cpp:122-186 restated with value arrays, 8-bit "
+                f"passes) on {threads} threads")
+
+        def step():
+            return _lsd_full(case, threads)[0]
+    for _ in range(min(args.warmup, 1)):
+        step()
+    budget_s = 150.0
+    t_end = time.perf_counter() + budget_s
+    times = []
+    for _ in range(args.steps):
+        times.append(step())
+        if time.perf_counter() > t_end:
+            break
     total = sum(times)
-    value = sample_n * len(times) / total / 1e6
+    value = case.n * len(times) / total / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(total / len(times) * 1e3, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": workload_config(case, args, {"sample": sample_n}),
-            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads,
-                             "kind": "port",
-                             "sample": f"first {sample_n} elements per step"},
+            "n_gpus": args.gpus, "steps": args.steps, "steps_timed": len(times),
+            "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded numpy MT19937)",
+            "config": workload_config(case, args),
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores,
+                             "kind": kind,
+                             "sample": f"the whole workload per step ({case.n} elements), "
+                                       f"{what}"},
             "e2e": {"value": round(value, 3), "unit": UNIT,
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -1097,7 +1192,7 @@ def main():
             "roofline": roofline,
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(case)
+        line["cpu_baseline"] = cpu_baseline(case, keys, vals)
     engine.release()
     reps.close()
     if rank == 0:

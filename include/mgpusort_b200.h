@@ -179,9 +179,14 @@ sortStatus_t SORTAPI sortServerDestroy(sortServer_t server);
  * numElements above SORT_NOALLOC_MAX_ELEMENTS returns
  * SORT_STATUS_CONFIG_NOT_SUPPORTED without device work.
  *
- * Every call shares the one array: calls whose work overlaps on the GPU (from
- * several host threads, or on several streams) race and corrupt each other's
- * results; issue them one after another. */
+ * Every call shares the one array, and calls whose work overlapped on the
+ * GPU would race on it. So that none can, a process-wide lock is held from
+ * the first launch until the sort has finished on the GPU: calls from several
+ * host threads (on any streams) run one after another, and a call waits for
+ * the one before it to finish. (Each process has its own copy of the array.)
+ * If a launch fails, the call returns SORT_STATUS_LAUNCH_ERROR and leaves the
+ * struct's buffers and parity as they were; the buffers' contents are then
+ * undefined. */
 sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t data, CUstream stream);
 
 #ifdef __cplusplus

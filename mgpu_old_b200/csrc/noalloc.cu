@@ -161,21 +161,29 @@ extern "C" sortStatus_t SORTAPI sortArrayNoAlloc(sortData_t d, CUstream cuStream
 	for(int i = 0; i < numArrays; ++i)
 		for(int j = 0; j < 2; ++j) bulk = bulk && (d->values[i][j] & 15) == 0;
 
+	// The passes ping-pong between the two buffers of a local copy of the
+	// caller's struct; the caller's struct takes the swaps only once every
+	// pass has been launched, so a launch failure leaves it as it was.
+	sortData_d work = *d;
 	cudaError_t ce = cudaSuccess;
 	for(int p = 0; p < passes; ++p) {
 		const int vm = (indexMode && p == 0) ? mgpusort::kValueIndex : numArrays;
 		mgpusort::PassBuffers buf = {};
-		buf.keysIn = reinterpret_cast<const unsigned*>(d->keys[0]);
-		buf.keysOut = reinterpret_cast<unsigned*>(d->keys[1]);
+		buf.keysIn = reinterpret_cast<const unsigned*>(work.keys[0]);
+		buf.keysOut = reinterpret_cast<unsigned*>(work.keys[1]);
 		for(int i = 0; i < 6; ++i) {
-			buf.valsIn[i] = reinterpret_cast<const unsigned*>(d->values[i][0]);
-			buf.valsOut[i] = reinterpret_cast<unsigned*>(d->values[i][1]);
+			buf.valsIn[i] = reinterpret_cast<const unsigned*>(work.values[i][0]);
+			buf.valsOut[i] = reinterpret_cast<unsigned*>(work.values[i][1]);
 		}
 		ce = mgpusort::launch_pass(buf, vm, n, p, plan, ctrl, passScratch, bulk, -1,
 			nullptr, s.numSMs, stream);
-		if(ce != cudaSuccess) return SORT_STATUS_LAUNCH_ERROR;
-		swap_buffers(d);
+		if(ce != cudaSuccess) {
+			cudaGetLastError();
+			return SORT_STATUS_LAUNCH_ERROR;
+		}
+		swap_buffers(&work);
 	}
+	for(int p = 0; p < passes; ++p) swap_buffers(d);
 
 	// Wait for the sort and read its device error word.
 	unsigned err = 0;

@@ -15,7 +15,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_cpusort.so")
 REF_BWT_LIB = os.path.join(HERE, "_ref", "libref_bwt.so")
-REFERENCE_TREE = "/root/reference"
+# Where the reference project's sources lie (read-only; only its CPU files
+# are compiled, by the Makefile's `ref` target). MGPU_REFERENCE_TREE
+# overrides the default location; where the tree is absent, the _ref/
+# libraries are not built and the tests pinned to them are skipped.
+REFERENCE_TREE = os.environ.get("MGPU_REFERENCE_TREE", "/root/reference")
 
 _u32p = POINTER(c_uint)
 

@@ -91,4 +91,32 @@ def test_reference_arm_json_line():
     assert line["cpu_baseline"]["kind"] in ("port", "reference")
     assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
-    assert line["config"]["workload"] == "pairs_and24_32M"
+    assert line["config"]["workload"] == "pairs_u32_64M"
+    assert line["config"]["n"] == 67_108_864       # the whole workload, no sample
+    assert line["steps_timed"] == 1
+
+
+@pytest.mark.parametrize("workload", ["keys_u32_1M", "pairs_and24_32M"])
+def test_reference_arm_never_loads_the_library(workload):
+    """The CPU arm runs the reference's CPU path only: after it, the process
+    has not mapped libmgpusort_b200.so."""
+    code = (
+        "import runpy, sys\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0',"
+        f" '--workload', '{workload}']\n"
+        "try:\n"
+        f"    runpy.run_path({os.path.join(ROOT, 'bench.py')!r}, run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED' if 'libmgpusort_b200' in maps else 'NOT_LOADED')\n")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr
+    out = p.stdout.strip().splitlines()
+    line = json.loads(out[-2])
+    assert line["impl"] == "reference" and line["config"]["workload"] == workload
+    have_ref = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_cpusort.so"))
+    expect_kind = "reference" if workload == "keys_u32_1M" and have_ref else "port"
+    assert line["cpu_baseline"]["kind"] == expect_kind
+    assert out[-1] == "NOT_LOADED"

@@ -46,6 +46,33 @@ def test_no_alloc_matches_sort_array_two_calls_in_a_row(engine):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("n,vc,fb,eb,offset,seed", [
+    (300_001, 1, 3, 9, 0, 4),      # one narrow pass
+    (250_007, 2, 0, 32, 1, 5),     # buffers 4 bytes past a 16-byte boundary: plain loads
+    (4_096, -1, 7, 25, 3, 6),      # index mode, unaligned, one tile
+])
+def test_no_alloc_against_oracle(engine, oracle_mod, n, vc, fb, eb, offset, seed):
+    """Bit-exact against the CPU oracle (std::stable_sort by the bit field),
+    twice in a row, including the path with plain loads for buffers that
+    are not 16-byte aligned."""
+    import torch
+    from mgpu_old_b200 import api
+    rng = np.random.Generator(np.random.MT19937(seed))
+    keys = _rand(rng, n)
+    keys[::3] &= np.uint32(0x0000FFF0)
+    vals = [_rand(rng, n) for _ in range(max(vc, 0))]
+    ek, ev = oracle_mod.sort_stable(keys, vals, vc, fb, eb)
+    for _ in range(2):
+        ds = DeviceSort(keys, vals, vc, fb, eb, offset=offset)
+        torch.cuda.synchronize()
+        st = api.sort_array_no_alloc(ds.data, 0)
+        assert st == api.SortStatus.SUCCESS, api.sort_status_string(st)
+        mk, mv = ds.result()
+        assert np.array_equal(mk, ek)
+        for a, b in zip(mv, ev):
+            assert np.array_equal(a, b)
+
+
 def test_no_alloc_index_mode_and_size_limit(engine):
     import torch
     from mgpu_old_b200 import api
