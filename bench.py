@@ -1166,7 +1166,9 @@ def main():
     alg_bytes = workloads.algorithmic_bytes(case.n, case.first_bit, case.end_bit,
                                             case.value_count)
     traffic = _ncu_traffic(case.name)
-    roofline = {"bound": "hbm", "kernel": "sort_kernel", "achieved": round(achieved, 1),
+    onesweep = os.environ.get("MGPU_SORT_PASS", "range") == "onesweep"
+    roofline = {"bound": "hbm", "kernel": "onesweep_kernel" if onesweep else "sort_kernel",
+                "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_src,
                 "traffic": traffic,
@@ -1174,7 +1176,8 @@ def main():
                 "whole_sort": {"alg_bytes": alg_bytes,
                                "achieved": round(alg_bytes / (ms_per_step * 1e-3) / 1e9, 1),
                                "frac": round(alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak, 4)},
-                "count_scan_avg_ms": round(kt["upsweep_ms"] / max(kt["upsweep_launches"], 1), 5),
+                ("upsweep_avg_ms" if onesweep else "count_scan_avg_ms"):
+                    round(kt["upsweep_ms"] / max(kt["upsweep_launches"], 1), 5),
                 "kernel_timing": "per-launch events in a second run of the same timed steps "
                                  f"({timed_ms / args.steps:.4f} ms per step with the events)"}
 
@@ -1186,9 +1189,12 @@ def main():
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "batches_in_flight": E2E_LANES,
                     "one_batch_at_a_time": round(e2e_serial, 1)},
-            # per pass: count + scan kernels (one timed "upsweep" entry) and
-            # the sort kernel
-            "gpu_launches": 2 * kt["upsweep_launches"] + kt["pass_launches"],
+            # onesweep: one upsweep per sort and one kernel per pass; range
+            # partition: count + scan kernels (one timed entry) and the sort
+            # kernel per pass
+            "gpu_launches": (1 if onesweep else 2) * kt["upsweep_launches"]
+                            + kt["pass_launches"],
+            "pass_method": "onesweep" if onesweep else "range",
             "roofline": roofline,
             "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

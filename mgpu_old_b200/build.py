@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(HERE, LIB_NAME)
 SOURCES = [
     "engine.cpp",
     "sort_kernels.cu",
+    "onesweep.cu",
     "noalloc.cu",
     "server.cpp",
     "bwt.cu",

@@ -28,6 +28,8 @@
 
 #include <cuda_runtime.h>
 
+#include "sort_common.cuh"
+
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -246,8 +248,8 @@ bwtStatus_t BWTAPI bwtSortBlock(bwtEngine_t engine, const void* block, int count
 	g.indices = array(kMaxStreams, 0);
 	const int grid = std::max(1, std::min(engine->numSMs * 8,
 		(count + kThreads - 1) / kThreads));
-	bwt_gather_keys<<<grid, kThreads, 0, stream>>>(g);
-	if(cudaGetLastError() != cudaSuccess) return BWT_STATUS_LAUNCH_ERROR;
+	if(mgpusort::launch_plain(bwt_gather_keys, grid, kThreads, 0, stream, g) != cudaSuccess)
+		return BWT_STATUS_LAUNCH_ERROR;
 
 	// Most significant stream last; the parity says which half of every
 	// array still carried holds its current contents (mgpusort.cpp:519-526).
@@ -276,9 +278,10 @@ bwtStatus_t BWTAPI bwtSortBlock(bwtEngine_t engine, const void* block, int count
 	}
 	const unsigned* sorted = reinterpret_cast<const unsigned*>(d.values[0][0]);
 
-	bwt_head_flags<<<grid, kThreads, 0, stream>>>(engine->dSym, sorted, count,
-		gpuKeySize, engine->dFlags);
-	if(cudaGetLastError() != cudaSuccess) return BWT_STATUS_LAUNCH_ERROR;
+	if(mgpusort::launch_plain(bwt_head_flags, grid, kThreads, 0, stream,
+		static_cast<const unsigned char*>(engine->dSym), sorted, count, gpuKeySize,
+		engine->dFlags) != cudaSuccess)
+		return BWT_STATUS_LAUNCH_ERROR;
 
 	std::vector<int>& order = engine->order;
 	std::vector<unsigned char>& flags = engine->flags;

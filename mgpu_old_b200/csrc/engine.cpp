@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -106,6 +108,15 @@ struct sortEngine_d {
 	// Segmented-sort scratch, grown on demand.
 	void* segScratch = nullptr;
 	size_t segScratchBytes = 0;
+	// Onesweep lookback buffers (two, for alternate executed passes), grown
+	// on demand: osStatusBytes each.
+	void* osStatus[2] = {nullptr, nullptr};
+	size_t osStatusBytes = 0;
+	// Pass method of sortArray: range partition (count, scan and sort
+	// launches per pass) or onesweep (one launch per pass, decoupled
+	// lookback). MGPU_SORT_PASS=onesweep in the environment at engine
+	// creation selects the latter.
+	bool onesweep = false;
 	// Host-mapped error word written by kernels, read without synchronizing.
 	volatile unsigned* hostError = nullptr;
 	unsigned* hostErrorDev = nullptr;
@@ -167,6 +178,7 @@ void destroy_engine(sortEngine_d* e) {
 	if(e->ctrl) cudaFree(e->ctrl);
 	if(e->scratch) cudaFree(e->scratch);
 	if(e->segScratch) cudaFree(e->segScratch);
+	if(e->osStatus[0]) cudaFree(e->osStatus[0]);
 	if(e->hostError) cudaFreeHost(const_cast<unsigned*>(e->hostError));
 	if(e->hostTrivial) cudaFreeHost(e->hostTrivial);
 	if(e->done) cudaEventDestroy(e->done);
@@ -218,9 +230,13 @@ bool make_plan(int firstBit, int numBits, int bitPass, mgpusort::PassPlan* plan)
 
 bool aligned16(CUdeviceptr p) { return (p & 15) == 0; }
 
-// Checks the status of a launch sequence.
+// Checks the status of a launch sequence. With MGPU_SORT_VERBOSE set in the
+// environment, a failed launch also names its CUDA error on stderr.
 sortStatus_t launch_status(cudaError_t e) {
 	if(e == cudaSuccess) return SORT_STATUS_SUCCESS;
+	if(std::getenv("MGPU_SORT_VERBOSE"))
+		std::fprintf(stderr, "mgpusort: launch failed: %s (%s)\n", cudaGetErrorName(e),
+			cudaGetErrorString(e));
 	return SORT_STATUS_LAUNCH_ERROR;
 }
 
@@ -267,6 +283,30 @@ void drop_graphs(sortEngine_d* e) {
 	for(auto& g : e->graphCache) cudaGraphExecDestroy(g.exec);
 	e->graphCache.clear();
 	e->seenOnce.clear();
+}
+
+// Makes the onesweep lookback buffers hold `bytes` bytes each. Growing them
+// moves them, so every cached graph (which holds their old address) is
+// dropped first.
+sortStatus_t ensure_onesweep_status(sortEngine_d* e, size_t bytes) {
+	if(bytes <= e->osStatusBytes) return SORT_STATUS_SUCCESS;
+	drop_graphs(e);
+	if(e->osStatus[0]) {
+		// Earlier sorts may still read the old buffers.
+		if(e->done) cudaEventSynchronize(e->done);
+		cudaFree(e->osStatus[0]);
+	}
+	e->osStatus[0] = e->osStatus[1] = nullptr;
+	e->osStatusBytes = 0;
+	void* p = nullptr;
+	if(cudaMalloc(&p, 2 * bytes) != cudaSuccess) {
+		cudaGetLastError();
+		return SORT_STATUS_DEVICE_ALLOC_FAILED;
+	}
+	e->osStatus[0] = p;
+	e->osStatus[1] = static_cast<char*>(p) + bytes;
+	e->osStatusBytes = bytes;
+	return SORT_STATUS_SUCCESS;
 }
 
 // Runs a launch sequence seq(d, stream, &swaps) on `stream`. A sequence whose
@@ -338,6 +378,89 @@ sortStatus_t run_sequence(sortEngine_d* e, sortData_d* d, const GraphKey& key,
 	return SORT_STATUS_SUCCESS;
 }
 
+// Small arrays: one CTA sorts the whole array through every pass of the plan
+// in shared memory (one launch). The result is written where the multi-pass
+// sequence would leave it (buffer numPasses & 1, in place when even) and the
+// struct takes the same swaps, so buffers and parity are as for any size.
+sortStatus_t small_sequence(sortEngine_d* e, sortData_d* sd, cudaStream_t st, int* swaps,
+	const mgpusort::PassPlan& plan, int n, bool indexMode, int numArrays, int keyType) {
+	const int out = plan.numPasses & 1;
+	mgpusort::PassBuffers buf = {};
+	buf.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+	buf.keysOut = reinterpret_cast<unsigned*>(sd->keys[out]);
+	for(int i = 0; i < 6; ++i) {
+		buf.valsIn[i] = reinterpret_cast<const unsigned*>(sd->values[i][0]);
+		buf.valsOut[i] = reinterpret_cast<unsigned*>(sd->values[i][out]);
+	}
+	const int slot = timing_begin(e, kTimedPass, st);
+	cudaError_t ce = mgpusort::launch_small_array(buf,
+		indexMode ? mgpusort::kValueIndex : numArrays, plan, n, st);
+	timing_end(e, slot, st);
+	e->failTile = -1;
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+	for(int p = 0; p < plan.numPasses; ++p) {
+		swap_buffers(sd);
+		++*swaps;
+	}
+	ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(sd->keys[0]), n,
+		keyType, false, st);
+	return launch_status(ce);
+}
+
+// The onesweep launch sequence of one sort: the upsweep (every pass's digit
+// offsets; clears the first lookback buffer and the tile counters), the
+// earlyExit read-back of single-digit passes, then one launch per executed
+// pass, and the key transform back.
+sortStatus_t onesweep_sequence(sortEngine_d* e, sortData_d* sd, cudaStream_t st,
+	int* swaps, const mgpusort::PassPlan& plan, int n, bool indexMode, int numArrays,
+	bool bulk, size_t statusBytes, int keyType) {
+	int slot = timing_begin(e, kTimedUpsweep, st);
+	cudaError_t ce = mgpusort::launch_onesweep_upsweep(
+		reinterpret_cast<const unsigned*>(sd->keys[0]), n, plan, e->ctrl, e->osStatus[0],
+		statusBytes, e->hostErrorDev, e->numSMs, st);
+	timing_end(e, slot, st);
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+	bool skip[mgpusort::kMaxPasses] = {};
+	if(sd->earlyExit) {
+		if(cudaMemcpyAsync(e->hostTrivial, e->ctrl->trivial,
+			sizeof(unsigned) * plan.numPasses, cudaMemcpyDeviceToHost, st)
+			!= cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+			e->dirty = true;
+			return SORT_STATUS_DEVICE_ERROR;
+		}
+		for(int p = 0; p < plan.numPasses; ++p) skip[p] = e->hostTrivial[p] != 0;
+	}
+	int exec = 0;
+	for(int p = 0; p < plan.numPasses; ++p) {
+		if(skip[p]) continue;
+		const int vm = (indexMode && exec == 0) ? mgpusort::kValueIndex : numArrays;
+		mgpusort::PassBuffers buf = {};
+		buf.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+		buf.keysOut = reinterpret_cast<unsigned*>(sd->keys[1]);
+		for(int i = 0; i < 6; ++i) {
+			buf.valsIn[i] = reinterpret_cast<const unsigned*>(sd->values[i][0]);
+			buf.valsOut[i] = reinterpret_cast<unsigned*>(sd->values[i][1]);
+		}
+		slot = timing_begin(e, kTimedPass, st);
+		ce = mgpusort::launch_onesweep_pass(buf, vm, n, p, exec, plan, e->ctrl,
+			e->osStatus, bulk, e->failTile, e->hostErrorDev, e->numSMs, st);
+		timing_end(e, slot, st);
+		e->failTile = -1;
+		if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+		swap_buffers(sd);
+		++*swaps;
+		++exec;
+	}
+	if(indexMode && exec == 0) {
+		// Every pass was skipped: the identity order still needs its indices.
+		ce = mgpusort::launch_iota(reinterpret_cast<unsigned*>(sd->values1[0]), n, st);
+		if(ce != cudaSuccess) return launch_status(ce);
+	}
+	ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(sd->keys[0]), n,
+		keyType, false, st);
+	return launch_status(ce);
+}
+
 // The whole sort of one sortData_d: validation, upsweep, the pass loop.
 // bitPass 0 selects sortArray's plan, 1..6 sortArrayEx's. Signed and float
 // keys (keyType) are mapped to their uint32 image in place before the first
@@ -379,10 +502,23 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 	for(int i = 0; i < numArrays; ++i)
 		for(int j = 0; j < 2; ++j) bulk = bulk && aligned16(d->values[i][j]);
 
+	// Onesweep: lookback buffers for this size (index mode and one value
+	// array share a tile size, so the first mode decides).
+	const int firstMode = indexMode ? mgpusort::kValueIndex : numArrays;
+	const size_t statusBytes = mgpusort::onesweep_status_bytes(n, firstMode);
+	if(e->onesweep) {
+		const sortStatus_t gs = ensure_onesweep_status(e, statusBytes);
+		if(gs != SORT_STATUS_SUCCESS) return gs;
+	}
+
 	auto seq = [&](sortData_d* sd, cudaStream_t st, int* swaps) -> sortStatus_t {
 		cudaError_t ce = mgpusort::launch_key_transform(
 			reinterpret_cast<unsigned*>(sd->keys[0]), n, keyType, true, st);
 		if(ce != cudaSuccess) return launch_status(ce);
+		if(n <= mgpusort::small_array_max_elements())
+			return small_sequence(e, sd, st, swaps, plan, n, indexMode, numArrays, keyType);
+		if(e->onesweep) return onesweep_sequence(e, sd, st, swaps, plan, n, indexMode,
+			numArrays, bulk, statusBytes, keyType);
 
 		// earlyExit: one upsweep builds every pass's digit histogram, one
 		// read-back of the per-pass "single digit" flags, then those passes
@@ -495,6 +631,7 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 	if(bytes > e->segScratchBytes) {
 		drop_graphs(e);
 		if(e->segScratch) cudaFree(e->segScratch);
+	if(e->osStatus[0]) cudaFree(e->osStatus[0]);
 		e->segScratch = nullptr;
 		e->segScratchBytes = 0;
 		if(cudaMalloc(&e->segScratch, bytes) != cudaSuccess) {
@@ -594,6 +731,8 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 	sortEngine_d* e = new sortEngine_d;
 	e->device = device;
 	e->numSMs = prop.multiProcessorCount;
+	if(const char* m = std::getenv("MGPU_SORT_PASS"))
+		e->onesweep = std::strcmp(m, "onesweep") == 0;
 	sortStatus_t status = SORT_STATUS_SUCCESS;
 	void* p = nullptr;
 	if(mgpusort::configure_kernels() != cudaSuccess)
@@ -628,6 +767,10 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 			status = SORT_STATUS_HOST_ALLOC_FAILED;
 		e->hostTrivial = static_cast<unsigned*>(h);
 	}
+#ifdef MGPU_OS_STATUS_PREALLOC
+	if(status == SORT_STATUS_SUCCESS)
+		status = ensure_onesweep_status(e, mgpusort::onesweep_status_bytes(MGPU_OS_STATUS_PREALLOC, 2));
+#endif
 	if(status == SORT_STATUS_SUCCESS &&
 		(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess ||
 		cudaStreamCreateWithFlags(&e->captureStream, cudaStreamNonBlocking) != cudaSuccess))

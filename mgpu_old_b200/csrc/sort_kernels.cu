@@ -23,55 +23,17 @@
 
 #include "sort_kernels.h"
 #include "sort_device.cuh"
+#include "sort_common.cuh"
 #include "tile_config.h"
 
 #include <algorithm>
 
 namespace mgpusort {
 
-// Programmatic dependent launch: the count, scan and sort kernels of the
-// passes are launched so that each may be scheduled while its predecessor
-// in the stream drains. Each waits (griddepcontrol.wait) for the
-// predecessor to complete, with its memory visible, before touching global
-// memory. Count and scan then let their successor launch at once; the sort
-// kernel releases its successor when it exits. Launched without the
-// attribute (or after a non-kernel stream operation) the wait returns at
-// once.
-__device__ __forceinline__ void wait_for_predecessor() {
-	asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
-__device__ __forceinline__ void allow_successor() {
-	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-// carveout >= 0 also sets this launch's preferred shared-memory carveout
-// (percent of the L1/shared capacity).
-template<typename Arg>
-static cudaError_t launch_dependent(void (*kernel)(Arg), int grid, int block,
-	size_t smem, cudaStream_t stream, const Arg& arg, int carveout = -1) {
-	cudaLaunchConfig_t cfg = {};
-	cfg.gridDim = dim3(grid);
-	cfg.blockDim = dim3(block);
-	cfg.dynamicSmemBytes = smem;
-	cfg.stream = stream;
-	cudaLaunchAttribute attr[2];
-	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-	attr[0].val.programmaticStreamSerializationAllowed = 1;
-	cfg.attrs = attr;
-	cfg.numAttrs = 1;
-	if(carveout >= 0) {
-		attr[1].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
-		attr[1].val.sharedMemCarveout = (unsigned)carveout;
-		cfg.numAttrs = 2;
-	}
-	return cudaLaunchKernelEx(&cfg, kernel, arg);
-}
-
 ////////////////////////////////////////////////////////////////////////////////
 // Upsweep: digit histograms of every pass in one read of the keys.
 
-constexpr int kUpThreads = 512;
+constexpr int kUpThreads = 1024;
 constexpr int kUpKeysPerThread = 16;
 constexpr int kUpChunk = kUpThreads * kUpKeysPerThread;
 
@@ -82,44 +44,50 @@ struct UpsweepArgs {
 	PassPlan plan;
 	Control* ctrl;
 	volatile unsigned* hostError;
+	// Onesweep sorts: the first executed pass's lookback buffer, cleared here
+	// (statusWords words), and the tile counters, zeroed here.
+	unsigned* status0;
+	size_t statusWords;
 };
 
-// Each bin of the upsweep's shared histogram has kUpCopies counters, one per
-// lane class (lane % kUpCopies), in consecutive words: lanes of a warp that
-// hit the same bin in one instruction mostly update different words (in
-// different banks), which keeps skewed digits from serialising the atomics.
-constexpr int kUpCopies = 4;
-
-__device__ __forceinline__ void count_digits(unsigned* hist,
-	const unsigned (&k)[kUpKeysPerThread], int nValid, int shift,
-	unsigned mask, int copy) {
-#pragma unroll
-	for(int i = 0; i < kUpKeysPerThread; ++i)
-		if(i < nValid)
-			atomicAdd(&hist[((k[i] >> shift) & mask) * kUpCopies + copy], 1u);
+// Shared memory of the upsweep: every bin of every pass has one counter per
+// lane (word bin * 32 + lane), so the 32 atomics of a warp instruction fall
+// in 32 different banks whatever the digits; warps share the columns.
+__host__ __device__ constexpr size_t upsweep_smem_bytes(int totalBins) {
+	return sizeof(unsigned) * 32 * (size_t)totalBins;
 }
 
-__global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
-	const UpsweepArgs a) {
-
-	__shared__ unsigned sHist[kMaxBins * kUpCopies];
+__global__ void __launch_bounds__(kUpThreads, 1) upsweep_kernel(const UpsweepArgs a) {
+	extern __shared__ __align__(128) unsigned sHist[];
 	__shared__ unsigned sScan[kUpThreads / 32];
 	__shared__ unsigned sLast;
 
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
-	const int copy = lane & (kUpCopies - 1);
 	const int totalBins = a.plan.totalBins;
 	const int numPasses = a.plan.numPasses;
 
-	for(int i = tid; i < totalBins * kUpCopies; i += kUpThreads) sHist[i] = 0;
+	for(int i = tid; i < totalBins * 32; i += kUpThreads) sHist[i] = 0;
+	if(a.status0) {
+		for(size_t i = (size_t)blockIdx.x * kUpThreads + tid; i < a.statusWords;
+			i += (size_t)gridDim.x * kUpThreads)
+			a.status0[i] = 0;
+		if(blockIdx.x == 0 && tid < kMaxPasses) a.ctrl->tileCounter[tid] = 0;
+	}
 	__syncthreads();
 
+	unsigned* myCol = sHist + lane;
 	auto count_all = [&](const unsigned (&k)[kUpKeysPerThread], int nValid) {
-		for(int p = 0; p < numPasses; ++p)
-			count_digits(sHist + a.plan.binBase[p] * kUpCopies, k, nValid,
-				a.plan.shift[p], (1u << a.plan.width[p]) - 1, copy);
+#pragma unroll 1
+		for(int p = 0; p < numPasses; ++p) {
+			const int shift = a.plan.shift[p];
+			const unsigned mask = (1u << a.plan.width[p]) - 1;
+			unsigned* col = myCol + a.plan.binBase[p] * 32;
+#pragma unroll
+			for(int i = 0; i < kUpKeysPerThread; ++i)
+				if(i < nValid) atomicAdd(&col[((k[i] >> shift) & mask) * 32], 1u);
+		}
 	};
 
 	// Full chunks with 16-byte loads, the next chunk's loads in flight while
@@ -173,11 +141,12 @@ __global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 	}
 	__syncthreads();
 
-	for(int i = tid; i < totalBins; i += kUpThreads) {
-		unsigned c = 0;
+	// Column sums: warp w sums bins w, w + 32, ...; lane l reads column l.
+	for(int b = warp; b < totalBins; b += kUpThreads / 32) {
+		unsigned v = sHist[b * 32 + lane];
 #pragma unroll
-		for(int j = 0; j < kUpCopies; ++j) c += sHist[i * kUpCopies + j];
-		if(c) atomicAdd(&a.ctrl->hist[i], c);
+		for(int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+		if(lane == 0 && v) atomicAdd(&a.ctrl->hist[b], v);
 	}
 	__threadfence();
 	__syncthreads();
@@ -193,15 +162,15 @@ __global__ void __launch_bounds__(kUpThreads, 3) upsweep_kernel(
 	for(int p = 0; p < numPasses; ++p) {
 		const int bins = 1 << a.plan.width[p];
 		unsigned* hist = a.ctrl->hist + a.plan.binBase[p];
-		unsigned c = 0;
-		if(tid < bins) c = ld_relaxed_u32(hist + tid);
-		unsigned incl = warp_inclusive_scan(c, lane);
+		unsigned v = 0;
+		if(tid < bins) v = ld_relaxed_u32(hist + tid);
+		unsigned incl = warp_inclusive_scan(v, lane);
 		if(lane == 31) sScan[warp] = incl;
-		int nonEmpty = __syncthreads_count(c != 0);
+		int nonEmpty = __syncthreads_count(v != 0);
 		unsigned prefix = 0;
 		for(int w = 0; w < warp; ++w) prefix += sScan[w];
 		if(tid < bins) {
-			a.ctrl->offsets[a.plan.binBase[p] + tid] = prefix + incl - c;
+			a.ctrl->offsets[a.plan.binBase[p] + tid] = prefix + incl - v;
 			hist[tid] = 0;
 		}
 		if(tid == 0) a.ctrl->trivial[p] = nonEmpty <= 1;
@@ -439,43 +408,6 @@ template<int VM> struct SortLayout {
 	static_assert(TILE < 65536, "ranks are packed in 16 bits");
 };
 
-// Peers of an 8-bit digit: the lanes of the warp whose digit equals this
-// lane's. The low BB bits of the digit are resolved by ballots and a lookup
-// table spread over the lanes: from the ballots of bits 0..3, lane l builds
-// the entry for low nibble l & 15, the set of lanes whose low nibble equals
-// it (nClear[k] is all ones where bit k of lane l is clear, so
-// ballot ^ nClear[k] is the set of lanes agreeing with that bit of l), and a
-// lane fetches the entry of its own nibble by shuffle. The remaining high
-// bits are resolved in one of two ways:
-//   BB = 8: four more ballots build a second 16-entry table for the high
-//           nibble; peers = low entry & high entry (two shuffles);
-//   BB = 5: a fifth ballot widens the table to 32 entries (bit 4 of the
-//           lane: blocks are one-dimensional, so threadIdx.x & 16), and
-//           match.any on the top three bits gives the rest;
-//   BB = 4: match.any on the high nibble.
-// All three return the same set; which is fastest depends on the value mode
-// and the array size and is a choice of the autotuner.
-template<int BB>
-__device__ __forceinline__ unsigned match_digit8(unsigned d,
-	const unsigned (&nClear)[4]) {
-	static_assert(BB == 4 || BB == 5 || BB == 8, "ballot bits: 4, 5 or 8");
-	unsigned lo = __ballot_sync(0xffffffffu, d & 1u) ^ nClear[0];
-#pragma unroll
-	for(int k = 1; k < 4; ++k) lo &= __ballot_sync(0xffffffffu, d & (1u << k)) ^ nClear[k];
-	if constexpr(BB == 8) {
-		unsigned hi = __ballot_sync(0xffffffffu, d & 16u) ^ nClear[0];
-#pragma unroll
-		for(int k = 1; k < 4; ++k) hi &= __ballot_sync(0xffffffffu, d & (16u << k)) ^ nClear[k];
-		return __shfl_sync(0xffffffffu, lo, d & 15u) & __shfl_sync(0xffffffffu, hi, d >> 4);
-	} else if constexpr(BB == 5) {
-		const unsigned nClear4 = (threadIdx.x & 16u) ? 0u : 0xffffffffu;
-		lo &= __ballot_sync(0xffffffffu, d & 16u) ^ nClear4;
-		return __match_any_sync(0xffffffffu, d >> 5) & __shfl_sync(0xffffffffu, lo, d & 31u);
-	} else {
-		return __match_any_sync(0xffffffffu, d >> 4) & __shfl_sync(0xffffffffu, lo, d & 15u);
-	}
-}
-
 // Stable warp rank of one item with digit d and peers (match_digit8): the
 // group of peers starts at the warp's running count of the digit, which the
 // highest peer then advances by the group's size. Returns
@@ -489,26 +421,6 @@ __device__ __forceinline__ unsigned count_item(unsigned d, unsigned peers,
 	__syncwarp();
 	return (d << 16) | (base + __popc(peers & ltMask));
 }
-
-__device__ __forceinline__ void stage_tile(unsigned* dst, const unsigned* src,
-	unsigned bytes, uint64_t* bar) {
-	mbar_arrive_expect_tx(bar, bytes);
-	bulk_load(dst, src, bytes, bar);
-}
-
-// The digit of a key. A whole byte (8-bit digit at a multiple of 8) is one
-// byte permute; any other field a shift and a mask.
-template<bool BYTE> struct DigitOf {
-	int shift;
-	unsigned mask;
-	unsigned sel;
-	__device__ __forceinline__ DigitOf(int s, int width)
-		: shift(s), mask((1u << width) - 1), sel(0x4440u | (unsigned)(s >> 3)) { }
-	__device__ __forceinline__ unsigned operator()(unsigned k) const {
-		if constexpr(BYTE) return __byte_perm(k, 0u, sel);
-		else return (k >> shift) & mask;
-	}
-};
 
 // Rank the staged tile's keys (warp-striped: item i of lane l in warp w is
 // tile element w*32*IPT + i*32 + l, so (item, lane) order is input order per
@@ -1506,6 +1418,41 @@ __global__ void __launch_bounds__(kSmallThreads) small_sort_kernel(const SmallSo
 	}
 }
 
+// A whole array of at most kSmallThreads * IPT elements, sorted by one CTA
+// through every pass in shared memory (sortArray on small arrays: one launch).
+template<int IPT>
+__global__ void __launch_bounds__(kSmallThreads) small_array_kernel(const SmallSortArgs a,
+	int n) {
+	constexpr int NT = kSmallThreads;
+	__shared__ unsigned sKeys[NT * IPT];
+	__shared__ unsigned sIdx[NT * IPT];
+	__shared__ unsigned sWarpHist[(NT / 32) * kDigitBins];
+	__shared__ unsigned sScan[32];
+	const int lane = threadIdx.x & 31;
+	const unsigned ltMask = lanemask_lt();
+	unsigned nClear[4];
+#pragma unroll
+	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
+	small_sort_segment<IPT>(a, 0, n, sKeys, sIdx, sWarpHist, sScan, ltMask, nClear);
+}
+
+int small_array_max_elements() { return MGPU_SORT_SMALL_ARRAY_MAX; }
+
+cudaError_t launch_small_array(const PassBuffers& buf, int valueMode, const PassPlan& plan,
+	int n, cudaStream_t stream) {
+	if(n <= 0 || n > kSegSmallMax || n > MGPU_SORT_SMALL_ARRAY_MAX) return cudaErrorInvalidValue;
+	SmallSortArgs a = {};
+	a.buf = buf;
+	a.plan = plan;
+	a.numArrays = valueMode > 0 ? valueMode : 0;
+	a.indexMode = valueMode == kValueIndex;
+	constexpr int NT = kSmallThreads;
+	if(n > 8 * NT) return launch_plain(small_array_kernel<16>, 1, NT, 0, stream, a, n);
+	if(n > 4 * NT) return launch_plain(small_array_kernel<8>, 1, NT, 0, stream, a, n);
+	if(n > 2 * NT) return launch_plain(small_array_kernel<4>, 1, NT, 0, stream, a, n);
+	return launch_plain(small_array_kernel<2>, 1, NT, 0, stream, a, n);
+}
+
 __global__ void iota_kernel(unsigned* out, int n) {
 	for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
 		i += (long long)gridDim.x * blockDim.x)
@@ -1556,6 +1503,9 @@ cudaError_t configure_kernels() {
 	if((r = set_sort_attributes<4>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<5>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<6>()) != cudaSuccess) e = r;
+	if((r = configure_onesweep_kernels()) != cudaSuccess) e = r;
+	if((r = cudaFuncSetAttribute(upsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		(int)upsweep_smem_bytes(kMaxBins))) != cudaSuccess) e = r;
 	return e;
 }
 
@@ -1575,6 +1525,13 @@ size_t pass_scratch_bytes() {
 cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
 	Control* ctrl, volatile unsigned* hostError, int numSMs,
 	cudaStream_t stream) {
+	return launch_onesweep_upsweep(keys, n, plan, ctrl, nullptr, 0, hostError, numSMs,
+		stream);
+}
+
+cudaError_t launch_onesweep_upsweep(const unsigned* keys, int n, const PassPlan& plan,
+	Control* ctrl, void* status0, size_t statusBytes, volatile unsigned* hostError,
+	int numSMs, cudaStream_t stream) {
 	UpsweepArgs a;
 	a.keys = keys;
 	a.n = n;
@@ -1582,11 +1539,13 @@ cudaError_t launch_upsweep(const unsigned* keys, int n, const PassPlan& plan,
 	a.plan = plan;
 	a.ctrl = ctrl;
 	a.hostError = hostError;
+	a.status0 = static_cast<unsigned*>(status0);
+	a.statusWords = statusBytes / sizeof(unsigned);
 	long long chunks = ((long long)n + kUpChunk - 1) / kUpChunk;
-	int grid = (int)std::min<long long>(chunks, (long long)numSMs * 3);
+	int grid = (int)std::min<long long>(chunks, (long long)numSMs);
 	if(grid < 1) grid = 1;
-	upsweep_kernel<<<grid, kUpThreads, 0, stream>>>(a);
-	return cudaGetLastError();
+	return launch_plain(upsweep_kernel, grid, kUpThreads, upsweep_smem_bytes(plan.totalBins),
+		stream, a);
 }
 
 // CTAs of the sort kernel that fit on one SM (occupancy), once per mode.
@@ -1799,8 +1758,7 @@ cudaError_t launch_seg_plan(const int* offsets, int numSegments, int n,
 	a.counters = x.counters;
 	a.devError = &ctrl->error;
 	a.hostError = hostError;
-	seg_plan_kernel<<<1, kPlanThreads, 0, stream>>>(a);
-	return cudaGetLastError();
+	return launch_plain(seg_plan_kernel, 1, kPlanThreads, 0, stream, a);
 }
 
 cudaError_t launch_seg_small(const PassBuffers& buf, int valueMode,
@@ -1817,14 +1775,14 @@ cudaError_t launch_seg_small(const PassBuffers& buf, int valueMode,
 	a.list = x.tinyList;
 	a.listIndex = 0;
 	a.work = kSegWorkSmall;
-	small_sort_kernel<kSegTinyMax / kSmallThreads><<<numSMs * 8, kSmallThreads, 0,
-		stream>>>(a);
+	cudaError_t e = launch_plain(small_sort_kernel<kSegTinyMax / kSmallThreads>, numSMs * 8,
+		kSmallThreads, 0, stream, a);
+	if(e != cudaSuccess) return e;
 	a.list = x.smallList;
 	a.listIndex = 1;
 	a.work = kSegWorkSmall + 1;
-	small_sort_kernel<kSegSmallMax / kSmallThreads><<<numSMs * 4, kSmallThreads, 0,
-		stream>>>(a);
-	return cudaGetLastError();
+	return launch_plain(small_sort_kernel<kSegSmallMax / kSmallThreads>, numSMs * 4,
+		kSmallThreads, 0, stream, a);
 }
 
 template<int VM>
@@ -1840,13 +1798,12 @@ static int seg_sort_ctas_per_sm() {
 }
 
 template<int VM>
-static void launch_seg_sort_vm(const SegSortArgs& a, int numSMs, cudaStream_t stream) {
+static cudaError_t launch_seg_sort_vm(const SegSortArgs& a, int numSMs, cudaStream_t stream) {
 	using L = SortLayout<VM>;
 	const int grid = numSMs * seg_sort_ctas_per_sm<VM>();
 	if(a.sort.width == 8 && (a.sort.shift & 7) == 0)
-		seg_sort_kernel<VM, true><<<grid, L::NT, L::kBytes, stream>>>(a);
-	else
-		seg_sort_kernel<VM, false><<<grid, L::NT, L::kBytes, stream>>>(a);
+		return launch_plain(seg_sort_kernel<VM, true>, grid, L::NT, L::kBytes, stream, a);
+	return launch_plain(seg_sort_kernel<VM, false>, grid, L::NT, L::kBytes, stream, a);
 }
 
 cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
@@ -1864,7 +1821,8 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
 	c.counts = x.counts;
 	c.work = kSegWork + 2 * pass;
-	seg_count_kernel<<<numSMs * 4, kCountThreads, 0, stream>>>(c);
+	cudaError_t e = launch_plain(seg_count_kernel, numSMs * 4, kCountThreads, 0, stream, c);
+	if(e != cudaSuccess) return e;
 
 	SegScanArgs q;
 	q.offsets = offsets;
@@ -1875,7 +1833,8 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	q.counts = x.counts;
 	q.rangeStart = x.rangeStart;
 	q.rangeTrivial = x.rangeTrivial;
-	seg_scan_kernel<<<numSMs * 8, 256, 0, stream>>>(q);
+	e = launch_plain(seg_scan_kernel, numSMs * 8, 256, 0, stream, q);
+	if(e != cudaSuccess) return e;
 
 	SegSortArgs a;
 	a.sort.buf = buf;
@@ -1897,24 +1856,22 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	a.rangeStart = x.rangeStart;
 	a.rangeTrivial = x.rangeTrivial;
 	switch(valueMode) {
-		case -1: launch_seg_sort_vm<-1>(a, numSMs, stream); break;
-		case 0: launch_seg_sort_vm<0>(a, numSMs, stream); break;
-		case 1: launch_seg_sort_vm<1>(a, numSMs, stream); break;
-		case 2: launch_seg_sort_vm<2>(a, numSMs, stream); break;
-		case 3: launch_seg_sort_vm<3>(a, numSMs, stream); break;
-		case 4: launch_seg_sort_vm<4>(a, numSMs, stream); break;
-		case 5: launch_seg_sort_vm<5>(a, numSMs, stream); break;
-		case 6: launch_seg_sort_vm<6>(a, numSMs, stream); break;
+		case -1: return launch_seg_sort_vm<-1>(a, numSMs, stream);
+		case 0: return launch_seg_sort_vm<0>(a, numSMs, stream);
+		case 1: return launch_seg_sort_vm<1>(a, numSMs, stream);
+		case 2: return launch_seg_sort_vm<2>(a, numSMs, stream);
+		case 3: return launch_seg_sort_vm<3>(a, numSMs, stream);
+		case 4: return launch_seg_sort_vm<4>(a, numSMs, stream);
+		case 5: return launch_seg_sort_vm<5>(a, numSMs, stream);
+		case 6: return launch_seg_sort_vm<6>(a, numSMs, stream);
 		default: return cudaErrorInvalidValue;
 	}
-	return cudaGetLastError();
 }
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream) {
 	if(n <= 0) return cudaSuccess;
 	int grid = (int)std::min<long long>(((long long)n + 255) / 256, 4096);
-	iota_kernel<<<grid, 256, 0, stream>>>(out, n);
-	return cudaGetLastError();
+	return launch_plain(iota_kernel, grid, 256, 0, stream, out, n);
 }
 
 // Order-preserving uint32 image of signed and float keys (the transform of
@@ -1940,8 +1897,8 @@ cudaError_t launch_key_transform(unsigned* keys, int n, int keyType, bool forwar
 	cudaStream_t stream) {
 	if(n <= 0 || keyType == kKeyUint32) return cudaSuccess;
 	int grid = (int)std::min<long long>(((long long)n + 255) / 256, 4096);
-	key_transform_kernel<<<grid, 256, 0, stream>>>(keys, n, keyType, forward ? 1 : 0);
-	return cudaGetLastError();
+	return launch_plain(key_transform_kernel, grid, 256, 0, stream, keys, n, keyType,
+		forward ? 1 : 0);
 }
 
 } // namespace mgpusort

@@ -25,7 +25,11 @@ struct Control {
 	unsigned trivial[kMaxPasses];
 	unsigned ticket;
 	unsigned error;
-	unsigned reserved[94];
+	// Tile counters of the onesweep passes (one per executed pass): each CTA
+	// draws its tile from the counter, in launch order. The upsweep zeroes
+	// them at the start of every sort.
+	unsigned tileCounter[kMaxPasses];
+	unsigned reserved[62];
 };
 
 // Digit layout of a sort: pass p sorts by bits [shift[p], shift[p] +
@@ -66,8 +70,10 @@ int pass_tile_elements(int valueMode);
 // Bytes of the pass scratch (kPassScratchWords words).
 size_t pass_scratch_bytes();
 
-// Configure kernel attributes (dynamic shared memory); call once per device.
+// Configure kernel attributes (dynamic shared memory) of every kernel,
+// onesweep's included; call once per device.
 cudaError_t configure_kernels();
+cudaError_t configure_onesweep_kernels();
 
 // Digit histograms of every pass of `plan` in one read of the keys, their
 // exclusive scans and the per-pass "single digit" flags (earlyExit).
@@ -118,6 +124,42 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	int numSMs, cudaStream_t stream);
 
 cudaError_t launch_iota(unsigned* out, int n, cudaStream_t stream);
+
+// Arrays of at most small_array_max_elements() elements: one CTA sorts the
+// whole array through every pass of `plan` in shared memory, from buf.*In
+// into buf.*Out (which may alias).
+int small_array_max_elements();
+cudaError_t launch_small_array(const PassBuffers& buf, int valueMode, const PassPlan& plan,
+	int n, cudaStream_t stream);
+
+// Onesweep passes (onesweep.cu): one launch per pass, with the digit offsets
+// of every pass from one upsweep and each tile's offsets from a decoupled
+// lookback over its predecessors' published digit counts.
+//
+// Elements per tile of the onesweep pass kernel for a value mode; all modes
+// of one sort (index mode, then one value array) share a tile size.
+int onesweep_tile_elements(int valueMode);
+
+// Bytes of one lookback buffer for n elements (tiles x 256 64-bit words);
+// the engine keeps two, used by alternate executed passes.
+size_t onesweep_status_bytes(int n, int valueMode);
+
+// The upsweep of a onesweep sort: every pass's digit histogram and exclusive
+// offsets and single-digit flags (as launch_upsweep), and it zeroes the
+// tile counters and the first `statusBytes` bytes (a multiple of 4) of
+// status0, the first executed pass's lookback buffer.
+cudaError_t launch_onesweep_upsweep(const unsigned* keys, int n, const PassPlan& plan,
+	Control* ctrl, void* status0, size_t statusBytes, volatile unsigned* hostError,
+	int numSMs, cudaStream_t stream);
+
+// One onesweep pass by the digit of plan pass `pass`, the `exec`-th executed
+// pass of the sort (0-based): it draws tiles from ctrl->tileCounter[exec],
+// looks back in status[exec & 1] and clears status[(exec + 1) & 1] for the
+// next executed pass.
+cudaError_t launch_onesweep_pass(const PassBuffers& buf, int valueMode, int n,
+	int pass, int exec, const PassPlan& plan, Control* ctrl, void* const status[2],
+	bool useBulk, int failTile, volatile unsigned* hostError, int numSMs,
+	cudaStream_t stream);
 
 // Key types with an order-preserving uint32 image (sortArrayTyped).
 constexpr int kKeyUint32 = 0;

@@ -157,7 +157,70 @@
 #ifndef MGPU_SORT_SEG_SHARED_CARVEOUT
 #define MGPU_SORT_SEG_SHARED_CARVEOUT 0
 #endif
+// sortArray on at most this many elements (up to 4096) sorts the whole array
+// in one CTA's shared memory through every pass (one launch); 0 turns that off.
+#ifndef MGPU_SORT_SMALL_ARRAY_MAX
+#define MGPU_SORT_SMALL_ARRAY_MAX 4096
+#endif
 // Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
 #ifndef MGPU_SORT_MAX_DIGIT_BITS
 #define MGPU_SORT_MAX_DIGIT_BITS 8
+#endif
+
+// Onesweep pass kernels (onesweep.cu): ranking threads (the block has one
+// more warp, which does the lookback), keys per thread and CTAs per SM of a
+// tile per class (keys only; index mode or one value array; two to six
+// value arrays), the warp ranking's ballot bits and batch per class, and
+// the staging slots (2: the next tile is copied in while the current one is
+// reordered and stored).
+#ifndef MGPU_OS_KEYS_THREADS
+#define MGPU_OS_KEYS_THREADS 256
+#endif
+#ifndef MGPU_OS_KEYS_ITEMS
+#define MGPU_OS_KEYS_ITEMS 16
+#endif
+#ifndef MGPU_OS_KEYS_MIN_BLOCKS
+#define MGPU_OS_KEYS_MIN_BLOCKS 3
+#endif
+#ifndef MGPU_OS_KEYS_SLOTS
+#define MGPU_OS_KEYS_SLOTS 2
+#endif
+#ifndef MGPU_OS_SINGLE_THREADS
+#define MGPU_OS_SINGLE_THREADS 384
+#endif
+#ifndef MGPU_OS_SINGLE_ITEMS
+#define MGPU_OS_SINGLE_ITEMS 20
+#endif
+#ifndef MGPU_OS_SINGLE_MIN_BLOCKS
+#define MGPU_OS_SINGLE_MIN_BLOCKS 2
+#endif
+#ifndef MGPU_OS_SINGLE_SLOTS
+#define MGPU_OS_SINGLE_SLOTS 1
+#endif
+#ifndef MGPU_OS_MULTI_THREADS
+#define MGPU_OS_MULTI_THREADS 256
+#endif
+#ifndef MGPU_OS_MULTI_ITEMS
+#define MGPU_OS_MULTI_ITEMS 12
+#endif
+#ifndef MGPU_OS_MULTI_MIN_BLOCKS
+#define MGPU_OS_MULTI_MIN_BLOCKS 2
+#endif
+#ifndef MGPU_OS_KEYS_BALLOT_BITS
+#define MGPU_OS_KEYS_BALLOT_BITS 5
+#endif
+#ifndef MGPU_OS_SINGLE_BALLOT_BITS
+#define MGPU_OS_SINGLE_BALLOT_BITS 5
+#endif
+#ifndef MGPU_OS_MULTI_BALLOT_BITS
+#define MGPU_OS_MULTI_BALLOT_BITS 5
+#endif
+#ifndef MGPU_OS_KEYS_RANK_BATCH
+#define MGPU_OS_KEYS_RANK_BATCH 8
+#endif
+#ifndef MGPU_OS_SINGLE_RANK_BATCH
+#define MGPU_OS_SINGLE_RANK_BATCH 10
+#endif
+#ifndef MGPU_OS_MULTI_RANK_BATCH
+#define MGPU_OS_MULTI_RANK_BATCH 6
 #endif
