@@ -506,7 +506,7 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 	// array share a tile size, so the first mode decides).
 	const int firstMode = indexMode ? mgpusort::kValueIndex : numArrays;
 	const size_t statusBytes = mgpusort::onesweep_status_bytes(n, firstMode);
-	if(e->onesweep) {
+	if(e->onesweep && n > mgpusort::small_array_max_elements()) {
 		const sortStatus_t gs = ensure_onesweep_status(e, statusBytes);
 		if(gs != SORT_STATUS_SUCCESS) return gs;
 	}
@@ -629,17 +629,23 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 
 	const size_t bytes = mgpusort::seg_scratch_bytes(n, numSegments);
 	if(bytes > e->segScratchBytes) {
+		// The old scratch may still be in use by this engine's last sort:
+		// wait for it before the memory goes back. Growth is geometric, so a
+		// stream of growing batches reallocates only a few times.
 		drop_graphs(e);
-		if(e->segScratch) cudaFree(e->segScratch);
-	if(e->osStatus[0]) cudaFree(e->osStatus[0]);
+		if(e->segScratch) {
+			if(e->done) cudaEventSynchronize(e->done);
+			cudaFree(e->segScratch);
+		}
 		e->segScratch = nullptr;
+		const size_t grown = std::max(bytes, 2 * e->segScratchBytes);
 		e->segScratchBytes = 0;
-		if(cudaMalloc(&e->segScratch, bytes) != cudaSuccess) {
+		if(cudaMalloc(&e->segScratch, grown) != cudaSuccess) {
 			cudaGetLastError();
 			e->segScratch = nullptr;
 			return SORT_STATUS_DEVICE_ALLOC_FAILED;
 		}
-		e->segScratchBytes = bytes;
+		e->segScratchBytes = grown;
 	}
 	if(e->dirty) {
 		if(cudaMemsetAsync(e->ctrl, 0, sizeof(mgpusort::Control), stream)
@@ -767,10 +773,6 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 			status = SORT_STATUS_HOST_ALLOC_FAILED;
 		e->hostTrivial = static_cast<unsigned*>(h);
 	}
-#ifdef MGPU_OS_STATUS_PREALLOC
-	if(status == SORT_STATUS_SUCCESS)
-		status = ensure_onesweep_status(e, mgpusort::onesweep_status_bytes(MGPU_OS_STATUS_PREALLOC, 2));
-#endif
 	if(status == SORT_STATUS_SUCCESS &&
 		(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) != cudaSuccess ||
 		cudaStreamCreateWithFlags(&e->captureStream, cudaStreamNonBlocking) != cudaSuccess))

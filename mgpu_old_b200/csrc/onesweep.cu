@@ -229,10 +229,8 @@ __device__ __forceinline__ void os_lookback_warp(const OsArgs& a, int tile, unsi
 						pending &= ~(1u << k);
 					} else {
 						j[k] -= (int)((w[k] >> 32) & 0x3fffffffu);
-#ifndef MGPU_OS_NO_SPAN
 						st_relaxed_u64(row + d, lookback_word(excl[k] + sReal[d],
 							(unsigned)(tile - j[k]), false));
-#endif
 					}
 				}
 			}
@@ -624,17 +622,11 @@ static cudaError_t launch_os_vm(const OsArgs& a, int numSMs, cudaStream_t stream
 	using L = OsLayout<VM>;
 	constexpr int bb = OsConfig<VM>::kBallotBits;
 	const int grid = (int)std::min<long long>(a.numTiles, (long long)numSMs * os_ctas_per_sm<VM>());
-#ifdef MGPU_OS_NO_PDL
-	if(a.width == 8 && (a.shift & 7) == 0)
-		return launch_plain(onesweep_kernel<VM, true, bb>, grid, L::NT, L::kBytes, stream, a);
-	return launch_plain(onesweep_kernel<VM, false, bb>, grid, L::NT, L::kBytes, stream, a);
-#else
 	if(a.width == 8 && (a.shift & 7) == 0)
 		return launch_dependent(onesweep_kernel<VM, true, bb>, grid, L::NT, L::kBytes,
 			stream, a);
 	return launch_dependent(onesweep_kernel<VM, false, bb>, grid, L::NT, L::kBytes,
 		stream, a);
-#endif
 }
 
 cudaError_t launch_onesweep_pass(const PassBuffers& buf, int valueMode, int n,
