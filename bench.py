@@ -1170,12 +1170,20 @@ def main():
     pass_bytes = 2 * case.n * 4 * (1 + arrays)
     pass_launches = max(kt["pass_launches"], 1)
     pass_ms = kt["pass_ms"] / pass_launches
-    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     alg_bytes = workloads.algorithmic_bytes(case.n, case.first_bit, case.end_bit,
                                             case.value_count)
-    traffic = _ncu_traffic(case.name)
     onesweep = os.environ.get("MGPU_SORT_PASS", "range") == "onesweep"
-    roofline = {"bound": "hbm", "kernel": "onesweep_kernel" if onesweep else "sort_kernel",
+    kernel = "onesweep_kernel" if onesweep else "sort_kernel"
+    # Mid-size and small arrays run the whole sort in one launch (the
+    # cooperative sort, or one CTA in shared memory): no count/scan launches
+    # and one timed launch per sort, whose algorithmic bytes are the whole
+    # sort's.
+    if kt["upsweep_launches"] == 0 and kt["pass_launches"] == args.steps:
+        kernel = "coop_sort_kernel" if case.n > 4096 else "small_array_kernel"
+        pass_bytes = alg_bytes
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    traffic = _ncu_traffic(case.name)
+    roofline = {"bound": "hbm", "kernel": kernel,
                 "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_src,

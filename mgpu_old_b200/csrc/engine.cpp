@@ -117,6 +117,11 @@ struct sortEngine_d {
 	// lookback). MGPU_SORT_PASS=onesweep in the environment at engine
 	// creation selects the latter.
 	bool onesweep = false;
+	// sortArray of more than the small-array limit and at most this many
+	// elements (keys only, index mode, one value array) runs every pass in
+	// one cooperative launch. MGPU_SORT_COOP_MAX in the environment at engine
+	// creation overrides the built-in limit (0: never).
+	int coopMax = 0;
 	// Host-mapped error word written by kernels, read without synchronizing.
 	volatile unsigned* hostError = nullptr;
 	unsigned* hostErrorDev = nullptr;
@@ -407,6 +412,33 @@ sortStatus_t small_sequence(sortEngine_d* e, sortData_d* sd, cudaStream_t st, in
 	return launch_status(ce);
 }
 
+// Mid-size arrays: every pass in one cooperative launch (count, scan and
+// sort phases separated by grid-wide barriers). Pass p writes buffer
+// (p + 1) & 1, so the result lies where the multi-pass sequence leaves it
+// and the struct takes the same swaps.
+sortStatus_t coop_sequence(sortEngine_d* e, sortData_d* sd, cudaStream_t st, int* swaps,
+	const mgpusort::PassPlan& plan, int n, bool indexMode, int numArrays, bool bulk,
+	int keyType) {
+	mgpusort::PassBuffers buf = {};
+	buf.keysIn = reinterpret_cast<const unsigned*>(sd->keys[0]);
+	buf.keysOut = reinterpret_cast<unsigned*>(sd->keys[1]);
+	buf.valsIn[0] = reinterpret_cast<const unsigned*>(sd->values[0][0]);
+	buf.valsOut[0] = reinterpret_cast<unsigned*>(sd->values[0][1]);
+	const int slot = timing_begin(e, kTimedPass, st);
+	cudaError_t ce = mgpusort::launch_coop_sort(buf,
+		indexMode ? mgpusort::kValueIndex : numArrays, n, plan, e->ctrl, e->scratch, bulk,
+		e->hostErrorDev, e->numSMs, st);
+	timing_end(e, slot, st);
+	if(ce != cudaSuccess) { e->dirty = true; return launch_status(ce); }
+	for(int p = 0; p < plan.numPasses; ++p) {
+		swap_buffers(sd);
+		++*swaps;
+	}
+	ce = mgpusort::launch_key_transform(reinterpret_cast<unsigned*>(sd->keys[0]), n,
+		keyType, false, st);
+	return launch_status(ce);
+}
+
 // The onesweep launch sequence of one sort: the upsweep (every pass's digit
 // offsets; clears the first lookback buffer and the tile counters), the
 // earlyExit read-back of single-digit passes, then one launch per executed
@@ -517,6 +549,10 @@ sortStatus_t sort_impl(sortEngine_d* e, sortData_d* d, int bitPass,
 		if(ce != cudaSuccess) return launch_status(ce);
 		if(n <= mgpusort::small_array_max_elements())
 			return small_sequence(e, sd, st, swaps, plan, n, indexMode, numArrays, keyType);
+		if(n <= e->coopMax && numArrays <= 1 && !sd->earlyExit && e->failTile < 0
+			&& !e->onesweep)
+			return coop_sequence(e, sd, st, swaps, plan, n, indexMode, numArrays, bulk,
+				keyType);
 		if(e->onesweep) return onesweep_sequence(e, sd, st, swaps, plan, n, indexMode,
 			numArrays, bulk, statusBytes, keyType);
 
@@ -739,6 +775,8 @@ sortStatus_t SORTAPI sortCreateEngine(const char* kernelPath,
 	e->numSMs = prop.multiProcessorCount;
 	if(const char* m = std::getenv("MGPU_SORT_PASS"))
 		e->onesweep = std::strcmp(m, "onesweep") == 0;
+	e->coopMax = mgpusort::coop_max_elements();
+	if(const char* m = std::getenv("MGPU_SORT_COOP_MAX")) e->coopMax = std::atoi(m);
 	sortStatus_t status = SORT_STATUS_SUCCESS;
 	void* p = nullptr;
 	if(mgpusort::configure_kernels() != cudaSuccess)

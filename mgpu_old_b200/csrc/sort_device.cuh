@@ -111,6 +111,23 @@ __device__ __forceinline__ uint4 ld_stream_u4(const uint4* p) {
 	return v;
 }
 
+// 16-byte load cached in L2 only: coherent with stores that other CTAs of
+// the same grid made before a grid-wide barrier.
+__device__ __forceinline__ uint4 ld_cg_u4(const uint4* p) {
+	uint4 v;
+	asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];"
+		: "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p) : "memory");
+	return v;
+}
+
+// Streaming load of data that no CTA of the running grid writes (NC), or a
+// coherent one of data written earlier in the same grid.
+template<bool NC>
+__device__ __forceinline__ uint4 ld_in_u4(const uint4* p) {
+	if constexpr(NC) return ld_stream_u4(p);
+	else return ld_cg_u4(p);
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
 	unsigned m;
 	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -222,17 +222,16 @@ struct CountArgs {
 // Each lane owns one copy of the histogram, interleaved so that bin b of
 // lane l is word b * 32 + l: every atomic of a warp falls in its own bank,
 // and lanes never share a counter (warps do, through the atomic).
-__global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a) {
-	__shared__ unsigned sHist[kDigitBins * 32];
-	wait_for_predecessor();
-	allow_successor();
+// The digit counts of range r (one CTA of NT threads; sHist holds
+// kDigitBins * 32 words). NC: the keys are not written by the running grid.
+template<bool NC, int NT = kCountThreads>
+__device__ __forceinline__ void count_range(const CountArgs& a, int r, unsigned* sHist) {
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
-	const int r = blockIdx.x;
 	const unsigned mask = (1u << a.width) - 1;
 	const int shift = a.shift;
 
-	for(int i = tid; i < kDigitBins * 32; i += kCountThreads) sHist[i] = 0;
+	for(int i = tid; i < kDigitBins * 32; i += NT) sHist[i] = 0;
 	__syncthreads();
 
 	const long long begin = (long long)a.split.first_tile(r) * a.tile;
@@ -251,20 +250,20 @@ __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a)
 		constexpr int U = 4;
 		int i = tid;
 		uint4 q[U];
-		bool have = i + (U - 1) * kCountThreads < nvec;
+		bool have = i + (U - 1) * NT < nvec;
 		if(have) {
 #pragma unroll
-			for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + i + u * kCountThreads);
+			for(int u = 0; u < U; ++u) q[u] = ld_in_u4<NC>(src + i + u * NT);
 		}
 		while(have) {
 			uint4 cur[U];
 #pragma unroll
 			for(int u = 0; u < U; ++u) cur[u] = q[u];
-			const int inext = i + U * kCountThreads;
-			const bool haveNext = inext + (U - 1) * kCountThreads < nvec;
+			const int inext = i + U * NT;
+			const bool haveNext = inext + (U - 1) * NT < nvec;
 			if(haveNext) {
 #pragma unroll
-				for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + inext + u * kCountThreads);
+				for(int u = 0; u < U; ++u) q[u] = ld_in_u4<NC>(src + inext + u * NT);
 			}
 #pragma unroll
 			for(int u = 0; u < U; ++u) {
@@ -276,8 +275,8 @@ __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a)
 			i = inext;
 			have = haveNext;
 		}
-		for(; i < nvec; i += kCountThreads) {
-			const uint4 q = ld_stream_u4(src + i);
+		for(; i < nvec; i += NT) {
+			const uint4 q = ld_in_u4<NC>(src + i);
 			add(q.x);
 			add(q.y);
 			add(q.z);
@@ -285,17 +284,24 @@ __global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a)
 		}
 		done = begin + 4ll * nvec;
 	}
-	for(long long e = done + tid; e < end; e += kCountThreads) add(a.keys[e]);
+	for(long long e = done + tid; e < end; e += NT) add(a.keys[e]);
 	__syncthreads();
 
 	// Sum the 32 copies of each bin: warp w sums bins w, w + 16, ...; lane l
 	// reads copy l of the bin, a warp reduction adds them up.
-	for(int b = tid >> 5; b < kDigitBins; b += kCountThreads / 32) {
+	for(int b = tid >> 5; b < kDigitBins; b += NT / 32) {
 		unsigned c = sHist[b * 32 + lane];
 #pragma unroll
 		for(int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
 		if(lane == 0) a.rangeCounts[(size_t)b * a.split.numRanges + r] = c;
 	}
+}
+
+__global__ void __launch_bounds__(kCountThreads) count_kernel(const CountArgs a) {
+	__shared__ unsigned sHist[kDigitBins * 32];
+	wait_for_predecessor();
+	allow_successor();
+	count_range<true>(a, blockIdx.x, sHist);
 }
 
 struct ScanArgs {
@@ -307,11 +313,8 @@ struct ScanArgs {
 
 // One CTA per digit, one thread per range (R <= kMaxRanges = 1024): the
 // exclusive scan of the digit's range counts and the digit's total.
-__global__ void __launch_bounds__(1024) scan_kernel(const ScanArgs a) {
-	__shared__ unsigned sWarp[32];
-	wait_for_predecessor();
-	allow_successor();
-	const int d = blockIdx.x;
+// Digit d's column: one thread per range (numRanges <= blockDim.x).
+__device__ __forceinline__ void scan_digit(const ScanArgs& a, int d, unsigned* sWarp) {
 	const int t = threadIdx.x;
 	const int lane = t & 31;
 	const int warp = t >> 5;
@@ -329,6 +332,13 @@ __global__ void __launch_bounds__(1024) scan_kernel(const ScanArgs a) {
 	}
 	__syncthreads();
 	if(t < R) a.rangeOffsets[(size_t)d * R + t] = sWarp[warp] + incl - v;
+}
+
+__global__ void __launch_bounds__(1024) scan_kernel(const ScanArgs a) {
+	__shared__ unsigned sWarp[32];
+	wait_for_predecessor();
+	allow_successor();
+	scan_digit(a, blockIdx.x, sWarp);
 }
 
 struct SortArgs {
@@ -388,24 +398,33 @@ template<int VM> struct SortLayout {
 	static constexpr int NW = NT / 32;
 	static constexpr int KSLOTS = SortConfig<VM>::kKeySlots;
 	static constexpr int NV = VM > 0 ? VM : 0;
+	// Vector stores (keys only, index mode, one value array): the reordered
+	// tile leaves up to 3 unused words before each digit's run, so that a
+	// run's shared-memory position and its global position agree mod 4.
+	static constexpr bool VEC = MGPU_SORT_VECTOR_STORES != 0 && VM <= 1;
+	static constexpr int PAD = VEC ? 3 * kDigitBins : 0;
+	// Words per reordered buffer (a key slot, the value buffer).
+	static constexpr int TILEP = TILE + PAD;
 	// Keys only: no value buffer. One value array (or the generated
 	// indices): one buffer, reordered in place. Two or more: a buffer of
 	// source positions, then one staging buffer per value array.
 	static constexpr int NVBUF = VM == 0 ? 0 : (NV >= 2 ? 1 + NV : 1);
+	// Per digit: the scatter offset (one word), or with vector stores the
+	// pair {global - shared offset, run start | run end << 16}.
+	static constexpr int kTableWords = VEC ? 2 * kDigitBins : kDigitBins;
 	// Word offsets into dynamic shared memory.
 	static constexpr int kKeys = 0;
-	static constexpr int kVals = kKeys + KSLOTS * TILE;
-	static constexpr int kWarpHist = kVals + NVBUF * TILE;
-	static constexpr int kDigStart = kWarpHist + NW * kDigitBins;
-	static constexpr int kCount = kDigStart + kDigitBins;
-	static constexpr int kRunning = kCount + kDigitBins;
+	static constexpr int kVals = kKeys + KSLOTS * TILEP;
+	static constexpr int kWarpHist = kVals + NVBUF * TILEP;
+	static constexpr int kRunning = kWarpHist + NW * kDigitBins;
 	static constexpr int kScatter = kRunning + kDigitBins;
-	static constexpr int kScan = kScatter + kDigitBins;
+	static constexpr int kScan = kScatter + kTableWords;
 	static constexpr int kBar = kScan + 32;          // 8-byte aligned: even
 	static constexpr int kWords = kBar + 2 * kNumBars;
 	static constexpr size_t kBytes = sizeof(unsigned) * kWords;
 	static_assert(kBar % 2 == 0, "mbarriers need 8-byte alignment");
-	static_assert(TILE < 65536, "ranks are packed in 16 bits");
+	static_assert(TILE % 4 == 0 && TILEP % 4 == 0, "16-byte aligned buffers");
+	static_assert(TILEP < 65536, "ranks and run bounds are packed in 16 bits");
 };
 
 // Stable warp rank of one item with digit d and peers (match_digit8): the
@@ -471,7 +490,11 @@ template<int VM> struct SortSmem {
 		  scatter(reinterpret_cast<int*>(base + L::kScatter)), scan(base + L::kScan),
 		  bar(reinterpret_cast<uint64_t*>(base + L::kBar)) { }
 	__device__ __forceinline__ unsigned* keys(int slot) const {
-		return smem + L::kKeys + slot * L::TILE;
+		return smem + L::kKeys + slot * L::TILEP;
+	}
+	// Vector stores: per digit {global - shared offset, start | end << 16}.
+	__device__ __forceinline__ int2* runs() const {
+		return reinterpret_cast<int2*>(scatter);
 	}
 	// Several value arrays: the source positions and staging buffer v.
 	__device__ __forceinline__ unsigned* positions() const { return vals; }
@@ -495,7 +518,7 @@ __device__ __forceinline__ void sort_setup(const SortSmem<VM>& sm) {
 // streaming copy of the keys and value arrays (index mode: the positions).
 // With 16-byte aligned buffers the aligned middle moves in 16-byte vectors,
 // every array's load of a step in flight before its stores.
-template<int VM>
+template<int VM, bool NC = true>
 __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 	long long end, long long indexBase) {
 	constexpr int NV = SortLayout<VM>::NV;
@@ -518,11 +541,11 @@ __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 		const long long nvec = (vecEnd - head) >> 2;
 		for(long long j = threadIdx.x; j < nvec; j += NT) {
 			const long long e = (v0 + j) << 2;
-			uint4 k = ld_stream_u4(reinterpret_cast<const uint4*>(a.buf.keysIn) + v0 + j);
+			uint4 k = ld_in_u4<NC>(reinterpret_cast<const uint4*>(a.buf.keysIn) + v0 + j);
 			uint4 vals[NV > 0 ? NV : 1];
 #pragma unroll
 			for(int v = 0; v < NV; ++v)
-				vals[v] = ld_stream_u4(reinterpret_cast<const uint4*>(a.buf.valsIn[v]) + v0 + j);
+				vals[v] = ld_in_u4<NC>(reinterpret_cast<const uint4*>(a.buf.valsIn[v]) + v0 + j);
 			reinterpret_cast<uint4*>(a.buf.keysOut)[v0 + j] = k;
 			if constexpr(VM == kValueIndex) {
 				const unsigned x = (unsigned)(e - indexBase);
@@ -538,15 +561,26 @@ __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 }
 
 // Once the warps of a tile have counted their digits (sm.warpHist): per
-// digit the tile's count and exclusive start, and for every warp the position
-// where its run of the digit begins in the reordered tile (digit start +
-// counts of the warps before it), written over the warp counts. Element p of
-// the reordered tile then belongs at scatter[digit] + p globally, and each
-// digit's running offset advances by the tile's real count (padding is only
-// ever in digit 255 and is not counted). One barrier inside; the caller
-// synchronizes before reading the results.
+// digit the start of its run in the reordered tile, and for every warp the
+// position where its part of the run begins (run start + counts of the
+// warps before it), written over the warp counts. Each digit's running
+// offset advances by the tile's real count (padding is only ever in digit
+// 255 and is not counted).
+//
+// Without gaps the runs are packed (run start = exclusive prefix of the
+// digit counts) and element p of the reordered tile belongs at
+// scatter[digit] + p globally. With gaps (vector stores) run d starts at the
+// first position at or after the end of run d - 1 that is congruent mod 4
+// to its global start running[d]; as run d - 1 itself started congruent to
+// running[d - 1], the gap before run d is
+//   (running[d] - running[d - 1] - count[d - 1]) mod 4,
+// known from digit d - 1 alone, so the starts are one prefix sum of
+// count + gap. The runs table then holds per digit the global - shared
+// offset and the run's [start, end) over its real elements. One barrier
+// inside; the caller synchronizes before reading the results.
 template<int VM>
-__device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int count) {
+__device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int count,
+	bool gaps) {
 	using L = SortLayout<VM>;
 	constexpr int NW = L::NW;
 	const int tid = threadIdx.x;
@@ -554,14 +588,30 @@ __device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int co
 	const int warp = tid >> 5;
 	unsigned c[NW];
 	unsigned tileTotal = 0;
+	unsigned g = 0;
 	if(tid < kDigitBins) {
 #pragma unroll
 		for(int w = 0; w < NW; ++w) {
 			c[w] = sm.warpHist[w * kDigitBins + tid];
 			tileTotal += c[w];
 		}
+		g = sm.running[tid];
 	}
-	const unsigned incl = warp_inclusive_scan(tileTotal, lane);
+	unsigned gap = 0;
+	if constexpr(L::VEC) {
+		// End of run d - 1 mod 4: from the neighbouring lane, or for the
+		// first lane of a warp from shared memory.
+		unsigned prevEnd = __shfl_up_sync(0xffffffffu, g + tileTotal, 1);
+		if(lane == 0 && tid > 0 && tid < kDigitBins) {
+			unsigned t = 0;
+#pragma unroll
+			for(int w = 0; w < NW; ++w) t += sm.warpHist[w * kDigitBins + tid - 1];
+			prevEnd = sm.running[tid - 1] + t;
+		}
+		if(tid == 0) prevEnd = 0;
+		if(gaps && tid < kDigitBins) gap = (g - prevEnd) & 3u;
+	}
+	const unsigned incl = warp_inclusive_scan(tileTotal + gap, lane);
 	if(lane == 31 && tid < kDigitBins) sm.scan[warp] = incl;
 	__syncthreads();
 	if(tid < kDigitBins) {
@@ -575,9 +625,65 @@ __device__ __forceinline__ void tile_digit_starts(const SortSmem<VM>& sm, int co
 			run += c[w];
 		}
 		const unsigned mine = tileTotal - (tid == kDigitBins - 1 ? L::TILE - count : 0);
-		const unsigned g = sm.running[tid];
-		sm.scatter[tid] = (int)(g - digStart);
+		if constexpr(L::VEC)
+			sm.runs()[tid] = make_int2((int)(g - digStart),
+				(int)(digStart | ((digStart + mine) << 16)));
+		else
+			sm.scatter[tid] = (int)(g - digStart);
 		sm.running[tid] = g + mine;
+	}
+}
+
+// Stores a reordered tile laid out with gaps (tile_digit_starts): thread t
+// takes the aligned 4-element chunks t, t + NT, ... of shared memory. A chunk
+// inside one digit run (its first key's run covers all four positions) goes
+// out as one 16-byte store per array, at a 16-byte aligned global address
+// since shared and global positions of a run agree mod 4; a chunk at a run
+// boundary stores each element that lies inside its own digit's run. Gap
+// words hold stale data and lie in no run, so they are never stored. Without
+// 16-byte aligned buffers the tile has no gaps and every element is stored
+// on its own.
+template<int VM, bool BYTE>
+__device__ __forceinline__ void store_runs(const SortArgs& a, const SortSmem<VM>& sm,
+	const unsigned* sKeys, int count, const DigitOf<BYTE>& digit) {
+	using L = SortLayout<VM>;
+	constexpr int NT = L::NT;
+	const int2* runs = sm.runs();
+	const unsigned* sVals = sm.vals;
+	const int tid = threadIdx.x;
+	auto store_one = [&](int q, unsigned k, unsigned v) {
+		const int2 r = runs[digit(k)];
+		if(q >= (r.y & 0xffff) && q < (int)((unsigned)r.y >> 16)) {
+			a.buf.keysOut[q + r.x] = k;
+			if constexpr(VM != 0) a.buf.valsOut[0][q + r.x] = v;
+		}
+	};
+	if(a.useBulk) {
+		// The last run ends after every other.
+		const int len = (int)((unsigned)runs[kDigitBins - 1].y >> 16);
+		for(int q = tid * 4; q < len; q += NT * 4) {
+			const uint4 k = *reinterpret_cast<const uint4*>(sKeys + q);
+			uint4 v = make_uint4(0u, 0u, 0u, 0u);
+			if constexpr(VM != 0) v = *reinterpret_cast<const uint4*>(sVals + q);
+			const int2 r = runs[digit(k.x)];
+			if(q >= (r.y & 0xffff) && q + 4 <= (int)((unsigned)r.y >> 16)) {
+				*reinterpret_cast<uint4*>(a.buf.keysOut + q + r.x) = k;
+				if constexpr(VM != 0)
+					*reinterpret_cast<uint4*>(a.buf.valsOut[0] + q + r.x) = v;
+			} else {
+				store_one(q, k.x, v.x);
+				store_one(q + 1, k.y, v.y);
+				store_one(q + 2, k.z, v.z);
+				store_one(q + 3, k.w, v.w);
+			}
+		}
+	} else {
+		for(int p = tid; p < count; p += NT) {
+			const unsigned k = sKeys[p];
+			const int dst = runs[digit(k)].x + p;
+			a.buf.keysOut[dst] = k;
+			if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+		}
 	}
 }
 
@@ -670,7 +776,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 		}
 		__syncthreads();
 
-		tile_digit_starts<VM>(sm, count);
+		tile_digit_starts<VM>(sm, count, a.useBulk);
 
 		// Every warp's keys leave shared memory for registers before the tile
 		// is reordered in place.
@@ -712,9 +818,11 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 		}
 		__syncthreads();
 
-		// Write each run to its global position: element p of the reordered
-		// tile goes to scatter[digit] + p; consecutive p, consecutive addresses.
-		if(count == TILE) {
+		// Write each run to its global position: consecutive positions of
+		// the reordered tile, consecutive addresses.
+		if constexpr(L::VEC) {
+			store_runs<VM, BYTE>(a, sm, sKeys, count, digit);
+		} else if(count == TILE) {
 #pragma unroll
 			for(int j = 0; j < IPT; ++j) {
 				const int p = j * NT + tid;
@@ -835,7 +943,7 @@ __device__ void sort_range_multi(const SortArgs& a, const SortSmem<VM>& sm,
 				ltMask, nClear, rank);
 		}
 		__syncthreads();
-		tile_digit_starts<VM>(sm, count);
+		tile_digit_starts<VM>(sm, count, false);
 
 		unsigned keys[IPT];
 #pragma unroll
@@ -916,21 +1024,17 @@ __device__ __forceinline__ void sort_range(const SortArgs& a, const SortSmem<VM>
 	else sort_range_single<VM, BYTE, BB>(a, sm, begin, end, indexBase, phase);
 }
 
-// One pass over a whole array: CTA r sorts range r of the split.
-template<int VM, bool BYTE, int BB>
-__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
-sort_kernel(const SortArgs a) {
+// Range r of one pass (the CTA of sort_kernel, or of the cooperative sort):
+// where each digit's keys start in the output, then a copy if the pass has
+// a single digit, else the tiles of the range. NC: the input was not written
+// by the running grid.
+template<int VM, bool BYTE, int BB, bool NC>
+__device__ __forceinline__ void sort_one_range(const SortArgs& a, unsigned* smem, int r) {
 	using L = SortLayout<VM>;
-	extern __shared__ __align__(128) unsigned smem[];
-	// The successor (the next pass's count) is released when this grid
-	// exits, not here: released early, its CTAs cost more than the launch
-	// latency they hide.
-	wait_for_predecessor();
 	const SortSmem<VM> sm(smem);
 	const int tid = threadIdx.x;
 	const int lane = tid & 31;
 	const int warp = tid >> 5;
-	const int r = blockIdx.x;
 	const int R = a.split.numRanges;
 	const long long begin = (long long)a.split.first_tile(r) * L::TILE;
 	const long long end = min((long long)a.n, (long long)a.split.first_tile(r + 1) * L::TILE);
@@ -947,13 +1051,26 @@ sort_kernel(const SortArgs a) {
 		sm.running[tid] = prefix + inclTotal - total + a.rangeOffsets[(size_t)tid * R + r];
 	}
 	if(nonEmpty <= 1) {
-		copy_range<VM>(a, begin, end, 0);
+		copy_range<VM, NC>(a, begin, end, 0);
 		return;
 	}
 	sort_setup<VM>(sm);
 	__syncthreads();
 	unsigned phase = 0;
 	sort_range<VM, BYTE, BB>(a, sm, begin, end, 0, phase);
+}
+
+// One pass over a whole array: CTA r sorts range r of the split.
+template<int VM, bool BYTE, int BB>
+__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
+sort_kernel(const SortArgs a) {
+	using L = SortLayout<VM>;
+	extern __shared__ __align__(128) unsigned smem[];
+	// The successor (the next pass's count) is released when this grid
+	// exits, not here: released early, its CTAs cost more than the launch
+	// latency they hide.
+	wait_for_predecessor();
+	sort_one_range<VM, BYTE, BB, true>(a, smem, blockIdx.x);
 }
 
 ////////////////////////////////////////////////////////////////////////////////
@@ -1504,6 +1621,7 @@ cudaError_t configure_kernels() {
 	if((r = set_sort_attributes<5>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<6>()) != cudaSuccess) e = r;
 	if((r = configure_onesweep_kernels()) != cudaSuccess) e = r;
+	if((r = configure_coop_kernels()) != cudaSuccess) e = r;
 	if((r = cudaFuncSetAttribute(upsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		(int)upsweep_smem_bytes(kMaxBins))) != cudaSuccess) e = r;
 	return e;
@@ -1679,6 +1797,208 @@ cudaError_t launch_pass(const PassBuffers& buf, int valueMode, int n,
 	if(e != cudaSuccess) return e;
 	return launch_pass_sort(buf, valueMode, n, pass, plan, ctrl, scratch, useBulk,
 		failTile, hostError, numSMs, stream);
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Cooperative sort: every pass of a mid-size sort in one launch.
+//
+// A pass of the range partition is three dependent launches (count, scan,
+// sort); for arrays of a few million keys each launch's fixed latency
+// (prologue, first copy, drain) costs more than its work. Here one grid of
+// co-resident CTAs (a cooperative launch: all CTAs run at once) runs the
+// same three phases per pass with grid-wide barriers between them: CTA r
+// counts range r, CTA r scans the columns of digits r, r + R, ..., CTA r
+// sorts range r. Barriers are bounded waits: a CTA that gives up reports
+// kErrBarrierTimeout and returns. Keys and values written by one pass are
+// read by the next through L2 (coherent loads, bulk copies after a proxy
+// fence), never through the non-coherent path.
+
+struct CoopArgs {
+	unsigned* keys[2];              // [0]: input of pass 0; passes alternate
+	unsigned* vals[2];
+	PassPlan plan;
+	RangeSplit split;
+	unsigned* rangeCounts;          // [256][R]
+	unsigned* rangeOffsets;         // [256][R]
+	unsigned* totals;               // [256]
+	unsigned* barrier;              // arrivals, zero at launch
+	unsigned* devError;
+	volatile unsigned* hostError;
+	int n;
+	int vecOk;
+	int useBulk;
+	int indexFirst;                 // the first pass writes indices (index mode)
+};
+
+// Grid-wide barrier number `gen` (1, 2, ...): every CTA adds one arrival and
+// waits for gen x gridDim.x of them. Thread 0's fences make the CTA's
+// earlier global writes visible before its arrival and order its later
+// loads and bulk copies after the other CTAs' writes. False if the wait ran
+// out (reported).
+__device__ __forceinline__ bool grid_barrier(const CoopArgs& a, unsigned gen) {
+	__shared__ int sOk;
+	__syncthreads();
+	if(threadIdx.x == 0) {
+		int ok = 1;
+		__threadfence();
+		atomicAdd(a.barrier, 1u);
+		const unsigned target = gen * gridDim.x;
+		WaitBudget budget;
+		while(ld_relaxed_u32(a.barrier) < target) {
+			if(!budget.poll()) {
+				report_error(a.devError, a.hostError, kErrBarrierTimeout);
+				ok = 0;
+				break;
+			}
+		}
+		__threadfence();
+		asm volatile("fence.proxy.async.global;" ::: "memory");
+		sOk = ok;
+	}
+	__syncthreads();
+	return sOk != 0;
+}
+
+template<int VM, int BB>
+__global__ void __launch_bounds__(SortLayout<VM>::NT, SortConfig<VM>::kMinBlocks)
+coop_sort_kernel(const CoopArgs a) {
+	static_assert(VM == 0 || VM == 1, "keys only or one value array");
+	using L = SortLayout<VM>;
+	static_assert(L::kWords >= kDigitBins * 32 + 32, "count and scan fit the sort's memory");
+	extern __shared__ __align__(128) unsigned smem[];
+	const int r = blockIdx.x;
+	const int R = a.split.numRanges;
+	unsigned gen = 0;
+	for(int p = 0; p < a.plan.numPasses; ++p) {
+		const int src = p & 1;
+		CountArgs c;
+		c.keys = a.keys[src];
+		c.n = a.n;
+		c.tile = L::TILE;
+		c.shift = a.plan.shift[p];
+		c.width = a.plan.width[p];
+		c.vecOk = a.vecOk;
+		c.split = a.split;
+		c.rangeCounts = a.rangeCounts;
+		count_range<false, L::NT>(c, r, smem);
+		if(!grid_barrier(a, ++gen)) return;
+
+		ScanArgs sc;
+		sc.rangeCounts = a.rangeCounts;
+		sc.rangeOffsets = a.rangeOffsets;
+		sc.totals = a.totals;
+		sc.numRanges = R;
+		for(int d = r; d < kDigitBins; d += gridDim.x) {
+			scan_digit(sc, d, smem);
+			__syncthreads();
+		}
+		if(!grid_barrier(a, ++gen)) return;
+
+		SortArgs sa;
+		sa.buf.keysIn = a.keys[src];
+		sa.buf.keysOut = a.keys[src ^ 1];
+		for(int i = 0; i < 6; ++i) {
+			sa.buf.valsIn[i] = i ? nullptr : a.vals[src];
+			sa.buf.valsOut[i] = i ? nullptr : a.vals[src ^ 1];
+		}
+		sa.rangeOffsets = a.rangeOffsets;
+		sa.totals = a.totals;
+		sa.devError = a.devError;
+		sa.hostError = a.hostError;
+		sa.split = a.split;
+		sa.n = a.n;
+		sa.shift = a.plan.shift[p];
+		sa.width = a.plan.width[p];
+		sa.useBulk = a.useBulk;
+		sa.failTile = -1;
+		if(VM == 1 && a.indexFirst && p == 0)
+			sort_one_range<kValueIndex, false, BB, false>(sa, smem, r);
+		else
+			sort_one_range<VM, false, BB, false>(sa, smem, r);
+		if(p + 1 < a.plan.numPasses && !grid_barrier(a, ++gen)) return;
+	}
+}
+
+template<int VM>
+static int coop_ctas_per_sm() {
+	static int perSM = 0;
+	if(!perSM) {
+		int v = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v,
+			coop_sort_kernel<VM, SortConfig<VM>::kBallotBits>, SortLayout<VM>::NT,
+			SortLayout<VM>::kBytes);
+		perSM = v > 0 ? v : 0;
+	}
+	return perSM;
+}
+
+template<int VM>
+static cudaError_t launch_coop_vm(CoopArgs& a, int numSMs, cudaStream_t stream) {
+	using L = SortLayout<VM>;
+	const int perSM = coop_ctas_per_sm<VM>();
+	if(perSM <= 0) return cudaErrorCooperativeLaunchTooLarge;
+	RangeSplit split;
+	split.numTiles = (int)(((long long)a.n + L::TILE - 1) / L::TILE);
+	long long ranges = std::min<long long>(split.numTiles, (long long)numSMs * perSM);
+	// One scan thread per range.
+	ranges = std::min<long long>(ranges, std::min(L::NT, kMaxRanges));
+	split.numRanges = (int)std::max<long long>(ranges, 1);
+	split.tilesLo = split.numTiles / split.numRanges;
+	split.extra = split.numTiles % split.numRanges;
+	a.split = split;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(split.numRanges);
+	cfg.blockDim = dim3(L::NT);
+	cfg.dynamicSmemBytes = L::kBytes;
+	cfg.stream = stream;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, coop_sort_kernel<VM, SortConfig<VM>::kBallotBits>, a);
+}
+
+cudaError_t configure_coop_kernels() {
+	cudaError_t e = cudaSuccess;
+	cudaError_t r;
+	const cudaFuncAttribute m = cudaFuncAttributeMaxDynamicSharedMemorySize;
+	if((r = cudaFuncSetAttribute(coop_sort_kernel<0, SortConfig<0>::kBallotBits>, m,
+		(int)SortLayout<0>::kBytes)) != cudaSuccess) e = r;
+	if((r = cudaFuncSetAttribute(coop_sort_kernel<1, SortConfig<1>::kBallotBits>, m,
+		(int)SortLayout<1>::kBytes)) != cudaSuccess) e = r;
+	return e;
+}
+
+int coop_max_elements() {
+	return MGPU_SORT_COOP_MAX_ELEMENTS;
+}
+
+cudaError_t launch_coop_sort(const PassBuffers& buf, int valueMode, int n,
+	const PassPlan& plan, Control* ctrl, unsigned* scratch, bool useBulk,
+	volatile unsigned* hostError, int numSMs, cudaStream_t stream) {
+	if(valueMode < -1 || valueMode > 1 || n <= 0) return cudaErrorInvalidValue;
+	cudaError_t e = cudaMemsetAsync(&ctrl->coopBarrier, 0, sizeof(unsigned), stream);
+	if(e != cudaSuccess) return e;
+	CoopArgs a;
+	a.keys[0] = const_cast<unsigned*>(buf.keysIn);
+	a.keys[1] = buf.keysOut;
+	a.vals[0] = const_cast<unsigned*>(buf.valsIn[0]);
+	a.vals[1] = buf.valsOut[0];
+	a.plan = plan;
+	a.rangeCounts = scratch;
+	a.rangeOffsets = scratch + (size_t)kDigitBins * kMaxRanges;
+	a.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
+	a.barrier = &ctrl->coopBarrier;
+	a.devError = &ctrl->error;
+	a.hostError = hostError;
+	a.n = n;
+	a.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0
+		&& (reinterpret_cast<size_t>(buf.keysOut) & 15) == 0;
+	a.useBulk = useBulk ? 1 : 0;
+	a.indexFirst = valueMode == kValueIndex ? 1 : 0;
+	if(valueMode == 0) return launch_coop_vm<0>(a, numSMs, stream);
+	return launch_coop_vm<1>(a, numSMs, stream);
 }
 
 // Segmented scratch: [counters][lists 5 x S][range table 4 x Rmax]

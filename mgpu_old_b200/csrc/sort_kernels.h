@@ -29,7 +29,10 @@ struct Control {
 	// draws its tile from the counter, in launch order. The upsweep zeroes
 	// them at the start of every sort.
 	unsigned tileCounter[kMaxPasses];
-	unsigned reserved[62];
+	// Arrivals at the grid-wide barriers of the cooperative sort (zeroed
+	// before each launch).
+	unsigned coopBarrier;
+	unsigned reserved[61];
 };
 
 // Digit layout of a sort: pass p sorts by bits [shift[p], shift[p] +
@@ -74,6 +77,18 @@ size_t pass_scratch_bytes();
 // onesweep's included; call once per device.
 cudaError_t configure_kernels();
 cudaError_t configure_onesweep_kernels();
+cudaError_t configure_coop_kernels();
+
+// Cooperative sort (keys only, index mode or one value array): every pass
+// of the plan in one launch of co-resident CTAs with grid-wide barriers
+// between the count, scan and sort phases. Pass 0 reads buf.*In and writes
+// buf.*Out, later passes alternate, so the result lies in buf.*Out after an
+// odd number of passes and in buf.*In after an even one. Zeroes
+// ctrl->coopBarrier first. Used for sorts of at most coop_max_elements().
+int coop_max_elements();
+cudaError_t launch_coop_sort(const PassBuffers& buf, int valueMode, int n,
+	const PassPlan& plan, Control* ctrl, unsigned* scratch, bool useBulk,
+	volatile unsigned* hostError, int numSMs, cudaStream_t stream);
 
 // Digit histograms of every pass of `plan` in one read of the keys, their
 // exclusive scans and the per-pass "single digit" flags (earlyExit).

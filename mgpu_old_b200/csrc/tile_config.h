@@ -84,6 +84,14 @@
 //              8  score 1.079  segments_small_50000 1.065
 #pragma once
 
+// 1: the one-array sort passes (keys only, index mode, one value array)
+// store their output in aligned 16-byte vectors where a digit run covers
+// them (the reordered tile is laid out so that shared and global positions
+// agree mod 4); 0: one 4-byte store per element.
+#ifndef MGPU_SORT_VECTOR_STORES
+#define MGPU_SORT_VECTOR_STORES 0
+#endif
+
 #ifndef MGPU_SORT_KEYS_THREADS
 #define MGPU_SORT_KEYS_THREADS 512
 #endif
@@ -96,8 +104,14 @@
 #ifndef MGPU_SORT_SINGLE_THREADS
 #define MGPU_SORT_SINGLE_THREADS 384
 #endif
+// With vector stores the gaps of the reordered tile cost 2 x 3 KB of shared
+// memory per CTA: 384 x 19 still fits two CTAs per SM.
 #ifndef MGPU_SORT_SINGLE_ITEMS
+#if MGPU_SORT_VECTOR_STORES
+#define MGPU_SORT_SINGLE_ITEMS 19
+#else
 #define MGPU_SORT_SINGLE_ITEMS 20
+#endif
 #endif
 #ifndef MGPU_SORT_SINGLE_MIN_BLOCKS
 #define MGPU_SORT_SINGLE_MIN_BLOCKS 2
@@ -161,6 +175,14 @@
 // in one CTA's shared memory through every pass (one launch); 0 turns that off.
 #ifndef MGPU_SORT_SMALL_ARRAY_MAX
 #define MGPU_SORT_SMALL_ARRAY_MAX 4096
+#endif
+// sortArray on more than SMALL_ARRAY_MAX and at most COOP_MAX_ELEMENTS keys
+// (keys only, index mode or one value array) runs every pass in one
+// cooperative launch; 0 turns that off. Off: on B200 it measured slower than
+// the three launches per pass at every size from 64 Ki to 16 Mi keys (1 Mi
+// keys: 72 us against 59 us).
+#ifndef MGPU_SORT_COOP_MAX_ELEMENTS
+#define MGPU_SORT_COOP_MAX_ELEMENTS 0
 #endif
 // Widest digit of sortArray's pass plan (1..8): ceil(bits / width) passes.
 #ifndef MGPU_SORT_MAX_DIGIT_BITS
