@@ -1403,11 +1403,11 @@ struct SmallSortArgs {
 // through every pass, then keys are written out and each value array is
 // permuted through shared memory by the final positions (index mode writes
 // the positions). Ends with a barrier.
-template<int IPT>
+template<int IPT, int NT = kSmallThreads>
 __device__ __forceinline__ void small_sort_segment(const SmallSortArgs& a, int begin,
 	int len, unsigned* sKeys, unsigned* sIdx, unsigned* sWarpHist, unsigned* sScan,
 	unsigned ltMask, const unsigned (&nClear)[4]) {
-	constexpr int NT = kSmallThreads;
+	static_assert(NT >= kDigitBins && NT % 32 == 0 && NT <= 1024, "one thread per digit");
 	constexpr int TILE = NT * IPT;
 	constexpr int NW = NT / 32;
 	const int tid = threadIdx.x;
@@ -1429,23 +1429,29 @@ __device__ __forceinline__ void small_sort_segment(const SmallSortArgs& a, int b
 			(IPT < kSmallRankBatch ? IPT : kSmallRankBatch)>(sKeys, sWarpHist + warp * kDigitBins, warpBase,
 			lane, len, digit, ltMask, nClear, rank);
 		__syncthreads();
+		// Thread d < 256: digit d's count over the warps, its start, and
+		// each warp's run start.
 		unsigned c[NW];
 		unsigned tileTotal = 0;
+		if(tid < kDigitBins) {
 #pragma unroll
-		for(int w = 0; w < NW; ++w) {
-			c[w] = sWarpHist[w * kDigitBins + tid];
-			tileTotal += c[w];
+			for(int w = 0; w < NW; ++w) {
+				c[w] = sWarpHist[w * kDigitBins + tid];
+				tileTotal += c[w];
+			}
 		}
 		const unsigned incl = warp_inclusive_scan(tileTotal, lane);
-		if(lane == 31) sScan[warp] = incl;
+		if(lane == 31 && tid < kDigitBins) sScan[warp] = incl;
 		__syncthreads();
-		unsigned prefix = 0;
-		for(int w = 0; w < warp; ++w) prefix += sScan[w];
-		unsigned run = prefix + incl - tileTotal;
+		if(tid < kDigitBins) {
+			unsigned prefix = 0;
+			for(int w = 0; w < warp; ++w) prefix += sScan[w];
+			unsigned run = prefix + incl - tileTotal;
 #pragma unroll
-		for(int w = 0; w < NW; ++w) {
-			sWarpHist[w * kDigitBins + tid] = run;
-			run += c[w];
+			for(int w = 0; w < NW; ++w) {
+				sWarpHist[w * kDigitBins + tid] = run;
+				run += c[w];
+			}
 		}
 		unsigned keys[IPT], idx[IPT];
 #pragma unroll
@@ -1535,26 +1541,58 @@ __global__ void __launch_bounds__(kSmallThreads) small_sort_kernel(const SmallSo
 	}
 }
 
-// A whole array of at most kSmallThreads * IPT elements, sorted by one CTA
-// through every pass in shared memory (sortArray on small arrays: one launch).
-template<int IPT>
-__global__ void __launch_bounds__(kSmallThreads) small_array_kernel(const SmallSortArgs a,
-	int n) {
-	constexpr int NT = kSmallThreads;
-	__shared__ unsigned sKeys[NT * IPT];
-	__shared__ unsigned sIdx[NT * IPT];
-	__shared__ unsigned sWarpHist[(NT / 32) * kDigitBins];
-	__shared__ unsigned sScan[32];
+// A whole array of at most NT * IPT elements, sorted by one CTA of NT
+// threads through every pass in shared memory (sortArray on small arrays:
+// one launch). Dynamic shared memory: keys and positions (NT * IPT words
+// each), the warp histograms, the scan words.
+template<int NT, int IPT>
+__host__ __device__ constexpr size_t small_array_smem_bytes() {
+	return sizeof(unsigned) * (2 * (size_t)NT * IPT + (NT / 32) * kDigitBins + 32);
+}
+
+template<int NT, int IPT>
+__global__ void __launch_bounds__(NT) small_array_kernel(const SmallSortArgs a, int n) {
+	extern __shared__ __align__(128) unsigned smem[];
+	unsigned* sKeys = smem;
+	unsigned* sIdx = sKeys + NT * IPT;
+	unsigned* sWarpHist = sIdx + NT * IPT;
+	unsigned* sScan = sWarpHist + (NT / 32) * kDigitBins;
 	const int lane = threadIdx.x & 31;
 	const unsigned ltMask = lanemask_lt();
 	unsigned nClear[4];
 #pragma unroll
 	for(int k = 0; k < 4; ++k) nClear[k] = ((lane >> k) & 1) ? 0u : 0xffffffffu;
-	small_sort_segment<IPT>(a, 0, n, sKeys, sIdx, sWarpHist, sScan, ltMask, nClear);
+	small_sort_segment<IPT, NT>(a, 0, n, sKeys, sIdx, sWarpHist, sScan, ltMask, nClear);
 }
 
 int small_array_max_elements() { return MGPU_SORT_SMALL_ARRAY_MAX; }
 
+template<int NT, int IPT>
+static cudaError_t launch_small_shape(const SmallSortArgs& a, int n, cudaStream_t stream) {
+	return launch_plain(small_array_kernel<NT, IPT>, 1, NT,
+		(int)small_array_smem_bytes<NT, IPT>(), stream, a, n);
+}
+
+static cudaError_t configure_small_array_kernels() {
+	cudaError_t e = cudaSuccess;
+	cudaError_t r;
+	const cudaFuncAttribute m = cudaFuncAttributeMaxDynamicSharedMemorySize;
+#define MGPU_SMALL_SHAPE(nt, ipt) \
+	if((r = cudaFuncSetAttribute(small_array_kernel<nt, ipt>, m, \
+		(int)small_array_smem_bytes<nt, ipt>())) != cudaSuccess) e = r;
+	MGPU_SMALL_SHAPE(256, 2)
+	MGPU_SMALL_SHAPE(256, 4)
+	MGPU_SMALL_SHAPE(256, 8)
+	MGPU_SMALL_SHAPE(256, 16)
+	MGPU_SMALL_SHAPE(512, 4)
+	MGPU_SMALL_SHAPE(1024, 4)
+#undef MGPU_SMALL_SHAPE
+	return e;
+}
+
+// The CTA grows with the array (up to MGPU_SORT_SMALL_ARRAY_THREADS threads)
+// before the keys per thread do: more warps rank in parallel, and each
+// warp's chain of counter updates stays short.
 cudaError_t launch_small_array(const PassBuffers& buf, int valueMode, const PassPlan& plan,
 	int n, cudaStream_t stream) {
 	if(n <= 0 || n > kSegSmallMax || n > MGPU_SORT_SMALL_ARRAY_MAX) return cudaErrorInvalidValue;
@@ -1563,11 +1601,14 @@ cudaError_t launch_small_array(const PassBuffers& buf, int valueMode, const Pass
 	a.plan = plan;
 	a.numArrays = valueMode > 0 ? valueMode : 0;
 	a.indexMode = valueMode == kValueIndex;
-	constexpr int NT = kSmallThreads;
-	if(n > 8 * NT) return launch_plain(small_array_kernel<16>, 1, NT, 0, stream, a, n);
-	if(n > 4 * NT) return launch_plain(small_array_kernel<8>, 1, NT, 0, stream, a, n);
-	if(n > 2 * NT) return launch_plain(small_array_kernel<4>, 1, NT, 0, stream, a, n);
-	return launch_plain(small_array_kernel<2>, 1, NT, 0, stream, a, n);
+	constexpr int kMaxThreads = MGPU_SORT_SMALL_ARRAY_THREADS;
+	if(n <= 512) return launch_small_shape<256, 2>(a, n, stream);
+	if(n <= 1024) return launch_small_shape<256, 4>(a, n, stream);
+	if(kMaxThreads >= 512 && n <= 2048) return launch_small_shape<512, 4>(a, n, stream);
+	if(kMaxThreads >= 1024) return launch_small_shape<1024, 4>(a, n, stream);
+	if(kMaxThreads >= 512) return launch_small_shape<512, 8>(a, n, stream);
+	if(n <= 2048) return launch_small_shape<256, 8>(a, n, stream);
+	return launch_small_shape<256, 16>(a, n, stream);
 }
 
 __global__ void iota_kernel(unsigned* out, int n) {
@@ -1622,6 +1663,7 @@ cudaError_t configure_kernels() {
 	if((r = set_sort_attributes<6>()) != cudaSuccess) e = r;
 	if((r = configure_onesweep_kernels()) != cudaSuccess) e = r;
 	if((r = configure_coop_kernels()) != cudaSuccess) e = r;
+	if((r = configure_small_array_kernels()) != cudaSuccess) e = r;
 	if((r = cudaFuncSetAttribute(upsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		(int)upsweep_smem_bytes(kMaxBins))) != cudaSuccess) e = r;
 	return e;

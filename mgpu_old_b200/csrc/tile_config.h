@@ -176,6 +176,10 @@
 #ifndef MGPU_SORT_SMALL_ARRAY_MAX
 #define MGPU_SORT_SMALL_ARRAY_MAX 4096
 #endif
+// Largest CTA of that sort (256, 512 or 1024 threads).
+#ifndef MGPU_SORT_SMALL_ARRAY_THREADS
+#define MGPU_SORT_SMALL_ARRAY_THREADS 1024
+#endif
 // sortArray on more than SMALL_ARRAY_MAX and at most COOP_MAX_ELEMENTS keys
 // (keys only, index mode or one value array) runs every pass in one
 // cooperative launch; 0 turns that off. Off: on B200 it measured slower than
