@@ -1160,6 +1160,41 @@ def main():
            [p.numpy().view(np.uint32) for p in pinned_out[last][1:]])
     e2e_value = case.n * world / (e2e_ms / args.steps * 1e-3) / 1e6
     e2e_serial = case.n * world / (e2e_serial_ms / max(2, args.steps // 4) * 1e-3) / 1e6
+
+    # The copies alone: one step's inputs in on one stream while another
+    # step's results go out on a second, no sort. Its rate bounds e2e.
+    def copies_only(reps=3):
+        (srt_a, _, _), (srt_b, _, _) = lanes[0], lanes[1]
+        sa, sb = torch.cuda.Stream(device), torch.cuda.Stream(device)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sa.wait_event(e0)
+        sb.wait_event(e0)
+        da, db = srt_a.data, srt_b.data
+        for _ in range(reps):
+            with torch.cuda.stream(sa):
+                srt_a.bufs[da.keys[0]][:case.n].copy_(pinned_in[0], non_blocking=True)
+                for i in range(len(case.values)):
+                    srt_a.bufs[da.values[i][0]][:case.n].copy_(pinned_in[1 + i],
+                                                               non_blocking=True)
+            with torch.cuda.stream(sb):
+                pinned_out[1][0].copy_(srt_b.bufs[db.keys[0]][:case.n], non_blocking=True)
+                for i in range(srt_b.arrays):
+                    pinned_out[1][1 + i].copy_(srt_b.bufs[db.values[i][0]][:case.n],
+                                               non_blocking=True)
+        cur = torch.cuda.current_stream(device)
+        for st in (sa, sb):
+            ev = torch.cuda.Event()
+            ev.record(st)
+            cur.wait_event(ev)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    copy_ms = max_over_ranks(copies_only())
+    copy_bound = case.n * world / (copy_ms * 1e-3) / 1e6
     for _, eng in extra:
         eng.release()
     del extra
@@ -1204,7 +1239,12 @@ def main():
             "config": workload_config(case, args),
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "batches_in_flight": E2E_LANES,
-                    "one_batch_at_a_time": round(e2e_serial, 1)},
+                    "one_batch_at_a_time": round(e2e_serial, 1),
+                    "copy_bound": {"value": round(copy_bound, 1), "unit": UNIT,
+                                   "ms_per_step": round(copy_ms, 4),
+                                   "frac": round(e2e_value / copy_bound, 4),
+                                   "what": "the step's H2D and D2H copies alone, both "
+                                           "directions at once, no sort"}},
             # onesweep: one upsweep per sort and one kernel per pass; range
             # partition: count + scan kernels (one timed entry) and the sort
             # kernel per pass
