@@ -1098,7 +1098,7 @@ constexpr int kSegCounters = kSegWorkSmall + 2;
 constexpr int kSegTinyMax = 512;
 constexpr int kSegSmallMax = 4096;
 constexpr int kSegMaxRangesPerSegment = 64;
-constexpr int kSegTilesPerRange = 4;
+constexpr int kSegTilesPerRange = MGPU_SORT_SEG_TILES_PER_RANGE;
 constexpr int kPlanThreads = 1024;
 
 // counters: [0] tiny segments, [1] small, [2] large, [3] ranges, [4] error.
@@ -1269,7 +1269,22 @@ __global__ void __launch_bounds__(kCountThreads) seg_count_kernel(const SegCount
 			for(int i = begin + tid; i < head; i += kCountThreads) add(a.keys[i]);
 			const uint4* src = reinterpret_cast<const uint4*>(a.keys + head);
 			const int nvec = max(0, (end - head) / 4);
-			for(int i = tid; i < nvec; i += kCountThreads) {
+			// Four independent 16-byte loads in flight per thread.
+			constexpr int U = 4;
+			int i = tid;
+			for(; i + (U - 1) * kCountThreads < nvec; i += U * kCountThreads) {
+				uint4 q[U];
+#pragma unroll
+				for(int u = 0; u < U; ++u) q[u] = ld_stream_u4(src + i + u * kCountThreads);
+#pragma unroll
+				for(int u = 0; u < U; ++u) {
+					add(q[u].x);
+					add(q[u].y);
+					add(q[u].z);
+					add(q[u].w);
+				}
+			}
+			for(; i < nvec; i += kCountThreads) {
 				const uint4 q = ld_stream_u4(src + i);
 				add(q.x);
 				add(q.y);

@@ -167,6 +167,11 @@
 #ifndef MGPU_SORT_CARVEOUT_MAX_ELEMENTS
 #define MGPU_SORT_CARVEOUT_MAX_ELEMENTS 1048576
 #endif
+// Tiles per range of a large segment (a segment gets at most 64 ranges):
+// the unit of work of the segmented count and sort kernels.
+#ifndef MGPU_SORT_SEG_TILES_PER_RANGE
+#define MGPU_SORT_SEG_TILES_PER_RANGE 4
+#endif
 // 1: the segmented sort's kernels all take the largest carveout.
 #ifndef MGPU_SORT_SEG_SHARED_CARVEOUT
 #define MGPU_SORT_SEG_SHARED_CARVEOUT 0
