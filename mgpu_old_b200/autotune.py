@@ -40,6 +40,13 @@ CLASSES = {
         "candidates": [(384, 20, 2), (512, 14, 2), (512, 16, 2), (384, 24, 2), (256, 20, 3)],
         "workloads": [("keys_u32", 1 << 20), ("keys_u32", 1 << 24), ("keys_u32", 1 << 26)],
     },
+    # Keys-only passes of MGPU_SORT_KEYS_LARGE_ELEMENTS keys or more.
+    "keys_large": {
+        "keys": ("MGPU_SORT_KEYS_LARGE_THREADS", "MGPU_SORT_KEYS_LARGE_ITEMS",
+                 "MGPU_SORT_KEYS_LARGE_MIN_BLOCKS"),
+        "candidates": [(256, 20, 3), (512, 14, 2), (384, 20, 2), (256, 16, 3)],
+        "workloads": [("keys_u32", 1 << 25), ("keys_u32", 1 << 26), ("keys_u32", 3 << 25)],
+    },
     "single": {
         "keys": ("MGPU_SORT_SINGLE_THREADS", "MGPU_SORT_SINGLE_ITEMS",
                  "MGPU_SORT_SINGLE_MIN_BLOCKS"),

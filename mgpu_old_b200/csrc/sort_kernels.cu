@@ -369,23 +369,34 @@ constexpr int kFaultBar = 7;
 // arrays multiply the write fronts (ranges x digits x arrays), and a front
 // is revisited only once per tile of its range, so partial sectors leave L2
 // before they are completed: one CTA of 768 x 8 per SM halves the ranges.
+//
+// Value mode kKeysLarge is the keys-only pass of sortArray on at least
+// MGPU_SORT_KEYS_LARGE_ELEMENTS keys: a tile shape of its own (the keys-only
+// shape that is fastest at 1 Mi keys is not the fastest at 64 Mi).
+constexpr int kKeysLarge = -2;
+__host__ __device__ constexpr bool keys_only(int vm) { return vm == 0 || vm == kKeysLarge; }
+
 template<int VM> struct SortConfig {
+	static constexpr bool kBig = VM == kKeysLarge;
 	static constexpr int kThreads = VM >= 2 ? MGPU_SORT_MULTI_THREADS
+		: kBig ? MGPU_SORT_KEYS_LARGE_THREADS
 		: VM == 0 ? MGPU_SORT_KEYS_THREADS : MGPU_SORT_SINGLE_THREADS;
 	static constexpr int kItems = VM >= 2 ? MGPU_SORT_MULTI_ITEMS
+		: kBig ? MGPU_SORT_KEYS_LARGE_ITEMS
 		: VM == 0 ? MGPU_SORT_KEYS_ITEMS : MGPU_SORT_SINGLE_ITEMS;
 	static constexpr int kMinBlocks = VM >= 2 ? MGPU_SORT_MULTI_MIN_BLOCKS
+		: kBig ? MGPU_SORT_KEYS_LARGE_MIN_BLOCKS
 		: VM == 0 ? MGPU_SORT_KEYS_MIN_BLOCKS : MGPU_SORT_SINGLE_MIN_BLOCKS;
 	// Digit bits resolved by ballots in the warp ranking (match_digit8);
 	// sortArray on at least kLargeElements keys uses kBallotBitsLarge.
 	static constexpr int kBallotBits = VM >= 2 ? MGPU_SORT_MULTI_BALLOT_BITS
-		: VM == 0 ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_BALLOT_BITS;
+		: keys_only(VM) ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_BALLOT_BITS;
 	static constexpr int kBallotBitsLarge = VM >= 2 ? MGPU_SORT_MULTI_BALLOT_BITS
-		: VM == 0 ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_LARGE_BALLOT_BITS;
+		: keys_only(VM) ? MGPU_SORT_KEYS_BALLOT_BITS : MGPU_SORT_SINGLE_LARGE_BALLOT_BITS;
 	static constexpr int kLargeElements = MGPU_SORT_SINGLE_LARGE_ELEMENTS;
 	// Items of a thread whose peers are found before their counter updates.
 	static constexpr int kRankBatch = VM >= 2 ? MGPU_SORT_MULTI_RANK_BATCH
-		: VM == 0 ? MGPU_SORT_KEYS_RANK_BATCH : MGPU_SORT_SINGLE_RANK_BATCH;
+		: keys_only(VM) ? MGPU_SORT_KEYS_RANK_BATCH : MGPU_SORT_SINGLE_RANK_BATCH;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
@@ -408,7 +419,7 @@ template<int VM> struct SortLayout {
 	// Keys only: no value buffer. One value array (or the generated
 	// indices): one buffer, reordered in place. Two or more: a buffer of
 	// source positions, then one staging buffer per value array.
-	static constexpr int NVBUF = VM == 0 ? 0 : (NV >= 2 ? 1 + NV : 1);
+	static constexpr int NVBUF = keys_only(VM) ? 0 : (NV >= 2 ? 1 + NV : 1);
 	// Per digit: the scatter offset (one word), or with vector stores the
 	// pair {global - shared offset, run start | run end << 16}.
 	static constexpr int kTableWords = VEC ? 2 * kDigitBins : kDigitBins;
@@ -655,7 +666,7 @@ __device__ __forceinline__ void store_runs(const SortArgs& a, const SortSmem<VM>
 		const int2 r = runs[digit(k)];
 		if(q >= (r.y & 0xffff) && q < (int)((unsigned)r.y >> 16)) {
 			a.buf.keysOut[q + r.x] = k;
-			if constexpr(VM != 0) a.buf.valsOut[0][q + r.x] = v;
+			if constexpr(!keys_only(VM)) a.buf.valsOut[0][q + r.x] = v;
 		}
 	};
 	if(a.useBulk) {
@@ -664,11 +675,11 @@ __device__ __forceinline__ void store_runs(const SortArgs& a, const SortSmem<VM>
 		for(int q = tid * 4; q < len; q += NT * 4) {
 			const uint4 k = *reinterpret_cast<const uint4*>(sKeys + q);
 			uint4 v = make_uint4(0u, 0u, 0u, 0u);
-			if constexpr(VM != 0) v = *reinterpret_cast<const uint4*>(sVals + q);
+			if constexpr(!keys_only(VM)) v = *reinterpret_cast<const uint4*>(sVals + q);
 			const int2 r = runs[digit(k.x)];
 			if(q >= (r.y & 0xffff) && q + 4 <= (int)((unsigned)r.y >> 16)) {
 				*reinterpret_cast<uint4*>(a.buf.keysOut + q + r.x) = k;
-				if constexpr(VM != 0)
+				if constexpr(!keys_only(VM))
 					*reinterpret_cast<uint4*>(a.buf.valsOut[0] + q + r.x) = v;
 			} else {
 				store_one(q, k.x, v.x);
@@ -682,7 +693,7 @@ __device__ __forceinline__ void store_runs(const SortArgs& a, const SortSmem<VM>
 			const unsigned k = sKeys[p];
 			const int dst = runs[digit(k)].x + p;
 			a.buf.keysOut[dst] = k;
-			if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+			if constexpr(!keys_only(VM)) a.buf.valsOut[0][dst] = sVals[p];
 		}
 	}
 }
@@ -829,7 +840,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 				const unsigned k = sKeys[p];
 				const int dst = sScatter[digit(k)] + p;
 				a.buf.keysOut[dst] = k;
-				if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+				if constexpr(!keys_only(VM)) a.buf.valsOut[0][dst] = sVals[p];
 			}
 		} else {
 #pragma unroll
@@ -839,7 +850,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 					const unsigned k = sKeys[p];
 					const int dst = sScatter[digit(k)] + p;
 					a.buf.keysOut[dst] = k;
-					if constexpr(VM != 0) a.buf.valsOut[0][dst] = sVals[p];
+					if constexpr(!keys_only(VM)) a.buf.valsOut[0][dst] = sVals[p];
 				}
 			}
 		}
@@ -1647,8 +1658,10 @@ static cudaError_t set_sort_attributes() {
 		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, false, bbLarge>, attr, bytes);
 		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true, bbLarge>, attr, bytes);
 	}
-	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
-	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
+	if constexpr(VM != kKeysLarge) {
+		if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
+		if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
+	}
 	return e;
 }
 
@@ -1670,6 +1683,7 @@ cudaError_t configure_kernels() {
 #endif
 	if((r = set_sort_attributes<-1>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<0>()) != cudaSuccess) e = r;
+	if((r = set_sort_attributes<kKeysLarge>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<1>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<2>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<3>()) != cudaSuccess) e = r;
@@ -1686,6 +1700,7 @@ cudaError_t configure_kernels() {
 
 int pass_tile_elements(int valueMode) {
 	switch(valueMode) {
+		case kKeysLarge: return SortLayout<kKeysLarge>::TILE;
 		case -1: return SortLayout<-1>::TILE;
 		case 0: return SortLayout<0>::TILE;
 		case 1: return SortLayout<1>::TILE;
@@ -1751,8 +1766,16 @@ static RangeSplit split_for(int n, int numSMs) {
 	return split;
 }
 
+// The tile class of a sortArray pass: keys-only passes over at least
+// MGPU_SORT_KEYS_LARGE_ELEMENTS keys take the large-array shape.
+static int pass_class(int valueMode, int n) {
+	return valueMode == 0 && (long long)n >= MGPU_SORT_KEYS_LARGE_ELEMENTS ? kKeysLarge
+		: valueMode;
+}
+
 static RangeSplit split_for_mode(int valueMode, int n, int numSMs) {
 	switch(valueMode) {
+		case kKeysLarge: return split_for<kKeysLarge>(n, numSMs);
 		case -1: return split_for<-1>(n, numSMs);
 		case 0: return split_for<0>(n, numSMs);
 		case 1: return split_for<1>(n, numSMs);
@@ -1767,12 +1790,13 @@ static RangeSplit split_for_mode(int valueMode, int n, int numSMs) {
 cudaError_t launch_pass_count(const PassBuffers& buf, int valueMode, int n,
 	int pass, const PassPlan& plan, unsigned* scratch, int numSMs,
 	cudaStream_t stream) {
-	const RangeSplit split = split_for_mode(valueMode, n, numSMs);
+	const int cls = pass_class(valueMode, n);
+	const RangeSplit split = split_for_mode(cls, n, numSMs);
 	unsigned* rangeCounts = scratch;
 	CountArgs c;
 	c.keys = buf.keysIn;
 	c.n = n;
-	c.tile = pass_tile_elements(valueMode);
+	c.tile = pass_tile_elements(cls);
 	c.shift = plan.shift[pass];
 	c.width = plan.width[pass];
 	c.vecOk = (reinterpret_cast<size_t>(buf.keysIn) & 15) == 0;
@@ -1826,13 +1850,15 @@ cudaError_t launch_pass_sort(const PassBuffers& buf, int valueMode, int n,
 	a.totals = scratch + 2 * (size_t)kDigitBins * kMaxRanges;
 	a.devError = &ctrl->error;
 	a.hostError = hostError;
-	a.split = split_for_mode(valueMode, n, numSMs);
+	const int cls = pass_class(valueMode, n);
+	a.split = split_for_mode(cls, n, numSMs);
 	a.n = n;
 	a.shift = plan.shift[pass];
 	a.width = plan.width[pass];
 	a.useBulk = useBulk ? 1 : 0;
 	a.failTile = failTile;
-	switch(valueMode) {
+	switch(cls) {
+		case kKeysLarge: return launch_sort_vm<kKeysLarge>(a, stream);
 		case -1: return launch_sort_vm<-1>(a, stream);
 		case 0: return launch_sort_vm<0>(a, stream);
 		case 1: return launch_sort_vm<1>(a, stream);

@@ -125,6 +125,23 @@
 #ifndef MGPU_SORT_MULTI_MIN_BLOCKS
 #define MGPU_SORT_MULTI_MIN_BLOCKS 1
 #endif
+// Keys-only passes of sortArray on at least KEYS_LARGE_ELEMENTS keys: their
+// own tile shape (the keys class above is tuned on 1 Mi keys). 256 x 20 with
+// three CTAs per SM against 512 x 14 x 2, whole sorts of uniform 32-bit
+// keys: 4% slower at 16 Mi, 2.2% faster at 32 Mi, 4.0% at 48 Mi, 4.7% at
+// 64 Mi, 5.5% at 96 Mi.
+#ifndef MGPU_SORT_KEYS_LARGE_THREADS
+#define MGPU_SORT_KEYS_LARGE_THREADS 256
+#endif
+#ifndef MGPU_SORT_KEYS_LARGE_ITEMS
+#define MGPU_SORT_KEYS_LARGE_ITEMS 20
+#endif
+#ifndef MGPU_SORT_KEYS_LARGE_MIN_BLOCKS
+#define MGPU_SORT_KEYS_LARGE_MIN_BLOCKS 3
+#endif
+#ifndef MGPU_SORT_KEYS_LARGE_ELEMENTS
+#define MGPU_SORT_KEYS_LARGE_ELEMENTS 33554432
+#endif
 // Digit bits the warp ranking resolves by ballots (8, 5 or 4); match.any
 // resolves the rest. Keys, single and multi classes as above; "small" is the
 // segmented sort's kernel for segments that fit one tile.

@@ -9,6 +9,8 @@ against the oracle, through the C ABI.
   * multi6_17bit_16M: 16,777,216 keys uniform in [0, 2^17) with six random
     value arrays, bits [0, 32).
   * pairs_u32_64M: 67,108,864 uniform 32-bit keys, value = index, bits [0, 32).
+  * keys_u32_64M: 67,108,864 uniform 32-bit keys, keys only (the keys-only
+    passes of at least 40 Mi keys run their own tile shape).
   * segments_10k: 10,000 lognormal segments (median 2048, sigma 2) through
     sortSegmentedArray, against one stable sort per segment.
 
@@ -90,6 +92,14 @@ def test_pairs_u32_64m(engine, oracle_mod):
     from mgpu_old_b200 import workloads
     case = workloads.pairs_uniform32()
     assert case.n == 67_108_864
+    _sort_and_compare(engine, case, oracle_mod)
+
+
+def test_keys_u32_64m(engine, oracle_mod):
+    # Keys only from 40 Mi keys on: the large-array tile class.
+    from mgpu_old_b200 import workloads
+    case = workloads.keys_uniform32_64m()
+    assert case.n == 67_108_864 and case.value_count == 0
     _sort_and_compare(engine, case, oracle_mod)
 
 
