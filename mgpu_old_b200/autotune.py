@@ -44,14 +44,14 @@ CLASSES = {
     "keys_large": {
         "keys": ("MGPU_SORT_KEYS_LARGE_THREADS", "MGPU_SORT_KEYS_LARGE_ITEMS",
                  "MGPU_SORT_KEYS_LARGE_MIN_BLOCKS"),
-        "candidates": [(256, 20, 3), (512, 14, 2), (384, 20, 2), (256, 16, 3)],
+        "candidates": [(256, 28, 3), (256, 20, 3), (256, 32, 2), (512, 14, 2), (384, 20, 2)],
         "workloads": [("keys_u32", 1 << 25), ("keys_u32", 1 << 26), ("keys_u32", 3 << 25)],
     },
     "single": {
         "keys": ("MGPU_SORT_SINGLE_THREADS", "MGPU_SORT_SINGLE_ITEMS",
                  "MGPU_SORT_SINGLE_MIN_BLOCKS"),
-        "candidates": [(384, 20, 2), (256, 20, 3), (512, 14, 2), (384, 16, 2),
-                       (256, 24, 2), (768, 10, 1)],
+        "candidates": [(256, 32, 2), (256, 30, 2), (384, 20, 2), (256, 20, 3), (512, 14, 2),
+                       (384, 16, 2), (256, 24, 2), (768, 10, 1)],
         "workloads": [("pairs_and24", 1 << 25), ("pairs_u32", 1 << 26), ("index_u32", 1 << 24)],
     },
     "multi": {
@@ -98,7 +98,7 @@ CLASSES = {
     },
     "single_batch": {
         "keys": ("MGPU_SORT_SINGLE_RANK_BATCH",),
-        "candidates": [(1,), (4,), (5,), (10,), (20,)],
+        "candidates": [(1,), (4,), (5,), (8,), (10,), (16,), (20,)],
         "workloads": [("pairs_and24", 1 << 25), ("pairs_u32", 1 << 26), ("index_u32", 1 << 24),
                       ("segments_lognormal", 10_000)],
     },

@@ -435,6 +435,8 @@ template<int VM> struct SortLayout {
 	static constexpr size_t kBytes = sizeof(unsigned) * kWords;
 	static_assert(kBar % 2 == 0, "mbarriers need 8-byte alignment");
 	static_assert(TILE % 4 == 0 && TILEP % 4 == 0, "16-byte aligned buffers");
+	static_assert(NT >= kDigitBins && NT % 32 == 0,
+		"the digit starts take one thread per digit");
 	static_assert(TILEP < 65536, "ranks and run bounds are packed in 16 bits");
 };
 

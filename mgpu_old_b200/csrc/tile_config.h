@@ -101,16 +101,23 @@
 #ifndef MGPU_SORT_KEYS_MIN_BLOCKS
 #define MGPU_SORT_KEYS_MIN_BLOCKS 2
 #endif
+// The single class was swept again by hand after the autotuner's run above,
+// over shapes it had not tried (whole sorts, Gkeys/s, 64 Mi uniform pairs /
+// 32 Mi 24-bit skewed pairs / the 10k-segment batch): 384 x 20 (the
+// autotuner's choice) 39.8 / 55.8 / 36.9; 256 x 32 41.4 / 57.9 / 36.3;
+// 256 x 30 40.1 / 57.5 / 35.8; 256 x 28 37.6 / 57.1 / 36.1; 352 x 22,
+// 320 x 24, 416 x 18 and 288 x 26 39.1-39.4 / 51.6-54.8. Fewer, longer warps
+// win. The ranking needs a thread per digit, so 256 threads is the floor.
 #ifndef MGPU_SORT_SINGLE_THREADS
-#define MGPU_SORT_SINGLE_THREADS 384
+#define MGPU_SORT_SINGLE_THREADS 256
 #endif
 // With vector stores the gaps of the reordered tile cost 2 x 3 KB of shared
-// memory per CTA: 384 x 19 still fits two CTAs per SM.
+// memory per CTA: 256 x 28 still fits two CTAs per SM.
 #ifndef MGPU_SORT_SINGLE_ITEMS
 #if MGPU_SORT_VECTOR_STORES
-#define MGPU_SORT_SINGLE_ITEMS 19
+#define MGPU_SORT_SINGLE_ITEMS 28
 #else
-#define MGPU_SORT_SINGLE_ITEMS 20
+#define MGPU_SORT_SINGLE_ITEMS 32
 #endif
 #endif
 #ifndef MGPU_SORT_SINGLE_MIN_BLOCKS
@@ -129,12 +136,13 @@
 // own tile shape (the keys class above is tuned on 1 Mi keys). 256 x 20 with
 // three CTAs per SM against 512 x 14 x 2, whole sorts of uniform 32-bit
 // keys: 4% slower at 16 Mi, 2.2% faster at 32 Mi, 4.0% at 48 Mi, 4.7% at
-// 64 Mi, 5.5% at 96 Mi.
+// 64 Mi, 5.5% at 96 Mi. At 64 Mi keys, 256 x 28 x 3 is 1.8% faster again
+// than 256 x 20 x 3 (256 x 32 x 2: 1.2%).
 #ifndef MGPU_SORT_KEYS_LARGE_THREADS
 #define MGPU_SORT_KEYS_LARGE_THREADS 256
 #endif
 #ifndef MGPU_SORT_KEYS_LARGE_ITEMS
-#define MGPU_SORT_KEYS_LARGE_ITEMS 20
+#define MGPU_SORT_KEYS_LARGE_ITEMS 28
 #endif
 #ifndef MGPU_SORT_KEYS_LARGE_MIN_BLOCKS
 #define MGPU_SORT_KEYS_LARGE_MIN_BLOCKS 3
@@ -170,8 +178,10 @@
 #ifndef MGPU_SORT_KEYS_RANK_BATCH
 #define MGPU_SORT_KEYS_RANK_BATCH 5
 #endif
+// With 256 x 32 tiles: batch 16 41.6 / 57.9, 10 41.4 / 57.9, 8 41.1 / 57.1
+// (Gkeys/s, 64 Mi pairs / 32 Mi skewed pairs).
 #ifndef MGPU_SORT_SINGLE_RANK_BATCH
-#define MGPU_SORT_SINGLE_RANK_BATCH 10
+#define MGPU_SORT_SINGLE_RANK_BATCH 16
 #endif
 #ifndef MGPU_SORT_MULTI_RANK_BATCH
 #define MGPU_SORT_MULTI_RANK_BATCH 8
