@@ -14,6 +14,7 @@
 #include "../../include/mgpusort.h"
 #include "../../include/mgpusort_b200.h"
 #pragma GCC visibility pop
+#include "engine_internal.h"
 #include "sort_kernels.h"
 #include "tile_config.h"
 
@@ -647,6 +648,29 @@ sortStatus_t validate(const sortData_d* d, bool* work) {
 	return SORT_STATUS_SUCCESS;
 }
 
+// Makes the segmented scratch hold `bytes` bytes. The old scratch may still
+// be in use by this engine's last sort: wait for it before the memory goes
+// back. Growth is geometric, so a stream of growing batches reallocates only
+// a few times.
+sortStatus_t ensure_seg_scratch(sortEngine_d* e, size_t bytes) {
+	if(bytes <= e->segScratchBytes) return SORT_STATUS_SUCCESS;
+	drop_graphs(e);
+	if(e->segScratch) {
+		if(e->done) cudaEventSynchronize(e->done);
+		cudaFree(e->segScratch);
+	}
+	e->segScratch = nullptr;
+	const size_t grown = std::max(bytes, 2 * e->segScratchBytes);
+	e->segScratchBytes = 0;
+	if(cudaMalloc(&e->segScratch, grown) != cudaSuccess) {
+		cudaGetLastError();
+		e->segScratch = nullptr;
+		return SORT_STATUS_DEVICE_ALLOC_FAILED;
+	}
+	e->segScratchBytes = grown;
+	return SORT_STATUS_SUCCESS;
+}
+
 sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 	int numSegments, cudaStream_t stream) {
 	if(!e || !d || !offsets || numSegments < 1) return SORT_STATUS_INVALID_VALUE;
@@ -663,26 +687,8 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 	if(!make_plan(d->firstBit, d->endBit - d->firstBit, 0, &plan))
 		return SORT_STATUS_INTERNAL_ERROR;
 
-	const size_t bytes = mgpusort::seg_scratch_bytes(n, numSegments);
-	if(bytes > e->segScratchBytes) {
-		// The old scratch may still be in use by this engine's last sort:
-		// wait for it before the memory goes back. Growth is geometric, so a
-		// stream of growing batches reallocates only a few times.
-		drop_graphs(e);
-		if(e->segScratch) {
-			if(e->done) cudaEventSynchronize(e->done);
-			cudaFree(e->segScratch);
-		}
-		e->segScratch = nullptr;
-		const size_t grown = std::max(bytes, 2 * e->segScratchBytes);
-		e->segScratchBytes = 0;
-		if(cudaMalloc(&e->segScratch, grown) != cudaSuccess) {
-			cudaGetLastError();
-			e->segScratch = nullptr;
-			return SORT_STATUS_DEVICE_ALLOC_FAILED;
-		}
-		e->segScratchBytes = grown;
-	}
+	const sortStatus_t gs = ensure_seg_scratch(e, mgpusort::seg_scratch_bytes(n, numSegments));
+	if(gs != SORT_STATUS_SUCCESS) return gs;
 	if(e->dirty) {
 		if(cudaMemsetAsync(e->ctrl, 0, sizeof(mgpusort::Control), stream)
 			!= cudaSuccess) return SORT_STATUS_DEVICE_ERROR;
@@ -743,6 +749,11 @@ sortStatus_t segmented_impl(sortEngine_d* e, sortData_d* d, const int* offsets,
 }
 
 } // namespace
+
+sortStatus_t engine_reserve_segmented(sortEngine_t engine, int n, int numSegments) {
+	if(!engine || n < 0 || numSegments < 1) return SORT_STATUS_INVALID_VALUE;
+	return ensure_seg_scratch(engine, mgpusort::seg_scratch_bytes(n, numSegments));
+}
 
 extern "C" {
 

@@ -12,6 +12,7 @@
 #include "../../include/mgpusort.h"
 #include "../../include/mgpusort_b200.h"
 #pragma GCC visibility pop
+#include "engine_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -302,6 +303,14 @@ sortStatus_t SORTAPI sortServerCreate(const sortServerConfig* config,
 		// their launch sequences seldom repeat, so slots launch directly
 		// rather than capture graphs.
 		sortEnableGraphs(slot.engine, 0);
+		// Scratch for the largest coalesced batch, now: growing it while
+		// serving would free device memory, which waits for every slot's work
+		// and stalls the scheduler.
+		st = engine_reserve_segmented(slot.engine, c.maxBatchElements, c.maxBatchRequests);
+		if(st != SORT_STATUS_SUCCESS) {
+			sortServerDestroy(s.release());
+			return st;
+		}
 		void* h = nullptr;
 		if(cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) != cudaSuccess ||
