@@ -120,3 +120,41 @@ def test_reference_arm_never_loads_the_library(workload):
     expect_kind = "reference" if workload == "keys_u32_1M" and have_ref else "port"
     assert line["cpu_baseline"]["kind"] == expect_kind
     assert out[-1] == "NOT_LOADED"
+
+
+@pytest.mark.parametrize("workload,metric,unit", [
+    ("segments_10k", "sort Mkeys/s", "Mkeys/s"),
+    ("multi6_17bit_16M", "sort Mkeys/s", "Mkeys/s"),
+    ("served", "sort Mkeys/s", "Mkeys/s"),
+    ("bwt", "bwtSortBlock MB/s", "MB/s"),
+])
+def test_reference_arm_other_workloads(workload, metric, unit):
+    """Every workload's reference arm prints one contract line (CPU only)
+    and never maps the library."""
+    code = (
+        "import runpy, sys\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0',"
+        f" '--workload', '{workload}']\n"
+        "try:\n"
+        f"    runpy.run_path({os.path.join(ROOT, 'bench.py')!r}, run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED' if 'libmgpusort_b200' in maps else 'NOT_LOADED')\n")
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr
+    out = p.stdout.strip().splitlines()
+    assert out[-1] == "NOT_LOADED"
+    line = json.loads(out[-2])
+    assert line["impl"] == "reference"
+    assert line["metric"] == metric and line["unit"] == unit
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    for key in ("n_gpus", "steps", "warmup", "ms_per_step", "scaling", "vs_baseline", "dtype",
+                "data", "config"):
+        assert key in line, key
+    cb = line["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1
+    assert cb["value"] == line["value"] and cb["unit"] == unit and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": unit, "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
