@@ -243,11 +243,13 @@
 #ifndef MGPU_OS_KEYS_SLOTS
 #define MGPU_OS_KEYS_SLOTS 2
 #endif
+// 256 x 32 (as the range sort's single class): 34.1 Gkeys/s for 64 Mi pairs
+// against 31.0 with 384 x 20 and 32.1 with 256 x 28.
 #ifndef MGPU_OS_SINGLE_THREADS
-#define MGPU_OS_SINGLE_THREADS 384
+#define MGPU_OS_SINGLE_THREADS 256
 #endif
 #ifndef MGPU_OS_SINGLE_ITEMS
-#define MGPU_OS_SINGLE_ITEMS 20
+#define MGPU_OS_SINGLE_ITEMS 32
 #endif
 #ifndef MGPU_OS_SINGLE_MIN_BLOCKS
 #define MGPU_OS_SINGLE_MIN_BLOCKS 2
