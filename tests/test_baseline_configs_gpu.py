@@ -12,7 +12,8 @@ against the oracle, through the C ABI.
   * keys_u32_64M: 67,108,864 uniform 32-bit keys, keys only (the keys-only
     passes of at least 40 Mi keys run their own tile shape).
   * segments_10k: 10,000 lognormal segments (median 2048, sigma 2) through
-    sortSegmentedArray, against one stable sort per segment.
+    sortSegmentedArray, against one stable sort per segment; also the same
+    sizes rescaled to 2^26 pairs in total.
 
 Inputs come from mgpu_old_b200.workloads, the generators the benchmark uses.
 Tolerance: exact (every key and every value array)."""
@@ -103,11 +104,15 @@ def test_keys_u32_64m(engine, oracle_mod):
     _sort_and_compare(engine, case, oracle_mod)
 
 
-def test_segments_10k_lognormal(engine, oracle_mod):
+@pytest.mark.parametrize("scale_to", [None, 1 << 26], ids=["unscaled", "total_64M"])
+def test_segments_10k_lognormal(engine, oracle_mod, scale_to):
     import torch
     from mgpu_old_b200 import api, workloads
-    case = workloads.segments_lognormal()
+    case = workloads.segments_lognormal(scale_to=scale_to)
     assert case.num_segments == 10_000
+    if scale_to:
+        # Rescaled sizes are rounded per segment: the total is within a few of 2^26.
+        assert abs(int(case.offsets[-1]) - scale_to) < 100
     ds = DeviceSort(case.keys, case.values, case.value_count, case.first_bit, case.end_bit)
     offs = torch.from_numpy(case.offsets.astype(np.int32)).cuda()
     torch.cuda.synchronize()
