@@ -11,9 +11,11 @@ steps; the restore copy and the flush are outside the timed region). `value`
 is device-resident throughput in Mkeys/s over the K timed steps (CUDA events
 on the sort's stream, max over ranks); `e2e` is the same metric through the C
 ABI with pinned host buffers, host->device and device->host copies inside the
-timed region. The roofline entry is the sort kernel of a pass (the dominant
-kernel), whose launches are timed with CUDA events inside the same timed
-steps (sortEnableKernelTiming).
+timed region, beside the bound that the copies alone set (`e2e.copy_bound`).
+The roofline entry is the sort kernel of a pass (the dominant kernel), whose
+launches are timed with CUDA events around each launch in a second run of the
+same timed steps (sortEnableKernelTiming), so that the events do not slow the
+run that gives `value`.
 
 Multi-GPU: the sort path does not shard (one global order), so N ranks run N
 independent replicas of the workload ("weak" scaling); the only collectives
