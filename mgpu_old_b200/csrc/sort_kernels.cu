@@ -2111,8 +2111,10 @@ constexpr int kMinTile = std::min({SortLayout<-1>::TILE, SortLayout<0>::TILE,
 // Ranges of a plan: a large segment (more than 4096 elements) of t tiles gets
 // min(64, ceil(t / 4)) ranges, and t <= len / tile + 2 (aligned-down start,
 // partial end), so it gets at most len / (4 tile) + 1.25. Summed over at most
-// n / 4096 large segments that is below n / tile + numSegments for any tile
-// up to 7680 keys (0.25 n / 4096 <= 0.75 n / tile).
+// n / 4096 large segments that is below n / kMinTile + numSegments (tile >=
+// kMinTile) whenever 0.25 n / 4096 <= 0.75 n / kMinTile, i.e. kMinTile <= 12288.
+static_assert(kMinTile <= 12288, "the range bound of seg_max_ranges");
+
 static size_t seg_max_ranges(int n, int numSegments) {
 	return (size_t)n / kMinTile + (size_t)numSegments + 1;
 }
