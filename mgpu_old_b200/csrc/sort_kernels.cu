@@ -375,17 +375,29 @@ constexpr int kFaultBar = 7;
 // shape that is fastest at 1 Mi keys is not the fastest at 64 Mi).
 constexpr int kKeysLarge = -2;
 __host__ __device__ constexpr bool keys_only(int vm) { return vm == 0 || vm == kKeysLarge; }
+// Value modes kSegOne (one value array) and kSegIndex (index mode) are those
+// of the segmented sort's range passes, which keep a tile shape of their own
+// (MGPU_SORT_SEG_SINGLE_*): their ranges are short, and the one-array
+// sortArray shape measured slower there.
+constexpr int kSegOne = -3;
+constexpr int kSegIndex = -4;
+__host__ __device__ constexpr bool seg_single(int vm) { return vm == kSegOne || vm == kSegIndex; }
+__host__ __device__ constexpr bool is_index(int vm) { return vm == kValueIndex || vm == kSegIndex; }
+__host__ __device__ constexpr int value_arrays(int vm) {
+	return vm == kSegOne ? 1 : (vm > 0 ? vm : 0);
+}
 
 template<int VM> struct SortConfig {
 	static constexpr bool kBig = VM == kKeysLarge;
+	static constexpr bool kSeg = seg_single(VM);
 	static constexpr int kThreads = VM >= 2 ? MGPU_SORT_MULTI_THREADS
-		: kBig ? MGPU_SORT_KEYS_LARGE_THREADS
+		: kBig ? MGPU_SORT_KEYS_LARGE_THREADS : kSeg ? MGPU_SORT_SEG_SINGLE_THREADS
 		: VM == 0 ? MGPU_SORT_KEYS_THREADS : MGPU_SORT_SINGLE_THREADS;
 	static constexpr int kItems = VM >= 2 ? MGPU_SORT_MULTI_ITEMS
-		: kBig ? MGPU_SORT_KEYS_LARGE_ITEMS
+		: kBig ? MGPU_SORT_KEYS_LARGE_ITEMS : kSeg ? MGPU_SORT_SEG_SINGLE_ITEMS
 		: VM == 0 ? MGPU_SORT_KEYS_ITEMS : MGPU_SORT_SINGLE_ITEMS;
 	static constexpr int kMinBlocks = VM >= 2 ? MGPU_SORT_MULTI_MIN_BLOCKS
-		: kBig ? MGPU_SORT_KEYS_LARGE_MIN_BLOCKS
+		: kBig ? MGPU_SORT_KEYS_LARGE_MIN_BLOCKS : kSeg ? MGPU_SORT_SEG_SINGLE_MIN_BLOCKS
 		: VM == 0 ? MGPU_SORT_KEYS_MIN_BLOCKS : MGPU_SORT_SINGLE_MIN_BLOCKS;
 	// Digit bits resolved by ballots in the warp ranking (match_digit8);
 	// sortArray on at least kLargeElements keys uses kBallotBitsLarge.
@@ -396,7 +408,8 @@ template<int VM> struct SortConfig {
 	static constexpr int kLargeElements = MGPU_SORT_SINGLE_LARGE_ELEMENTS;
 	// Items of a thread whose peers are found before their counter updates.
 	static constexpr int kRankBatch = VM >= 2 ? MGPU_SORT_MULTI_RANK_BATCH
-		: keys_only(VM) ? MGPU_SORT_KEYS_RANK_BATCH : MGPU_SORT_SINGLE_RANK_BATCH;
+		: keys_only(VM) ? MGPU_SORT_KEYS_RANK_BATCH
+		: kSeg ? MGPU_SORT_SEG_SINGLE_RANK_BATCH : MGPU_SORT_SINGLE_RANK_BATCH;
 	// Key tiles staged per CTA: with two, the next tile's keys are copied in
 	// while this tile is sorted.
 	static constexpr int kKeySlots = VM <= 1 ? 2 : 1;
@@ -408,7 +421,7 @@ template<int VM> struct SortLayout {
 	static constexpr int TILE = NT * IPT;
 	static constexpr int NW = NT / 32;
 	static constexpr int KSLOTS = SortConfig<VM>::kKeySlots;
-	static constexpr int NV = VM > 0 ? VM : 0;
+	static constexpr int NV = value_arrays(VM);
 	// Vector stores (keys only, index mode, one value array): the reordered
 	// tile leaves up to 3 unused words before each digit's run, so that a
 	// run's shared-memory position and its global position agree mod 4.
@@ -538,7 +551,7 @@ __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 	constexpr int NT = SortLayout<VM>::NT;
 	auto copy_one = [&](long long i) {
 		a.buf.keysOut[i] = a.buf.keysIn[i];
-		if constexpr(VM == kValueIndex) a.buf.valsOut[0][i] = (unsigned)(i - indexBase);
+		if constexpr(is_index(VM)) a.buf.valsOut[0][i] = (unsigned)(i - indexBase);
 #pragma unroll
 		for(int v = 0; v < NV; ++v) a.buf.valsOut[v][i] = a.buf.valsIn[v][i];
 	};
@@ -560,7 +573,7 @@ __device__ __forceinline__ void copy_range(const SortArgs& a, long long begin,
 			for(int v = 0; v < NV; ++v)
 				vals[v] = ld_in_u4<NC>(reinterpret_cast<const uint4*>(a.buf.valsIn[v]) + v0 + j);
 			reinterpret_cast<uint4*>(a.buf.keysOut)[v0 + j] = k;
-			if constexpr(VM == kValueIndex) {
+			if constexpr(is_index(VM)) {
 				const unsigned x = (unsigned)(e - indexBase);
 				reinterpret_cast<uint4*>(a.buf.valsOut[0])[v0 + j] =
 					make_uint4(x, x + 1, x + 2, x + 3);
@@ -805,7 +818,7 @@ __device__ void sort_range_single(const SortArgs& a, const SortSmem<VM>& sm,
 			rank[i] = (rank[i] & 0xffffu) + sWarpHist[warp * kDigitBins + (rank[i] >> 16)];
 			sKeys[rank[i]] = keys[i];
 		}
-		if constexpr(VM == kValueIndex) {
+		if constexpr(is_index(VM)) {
 #pragma unroll
 			for(int i = 0; i < IPT; ++i)
 				sVals[rank[i]] = (unsigned)(tileStart - indexBase + warpBase + i * 32 + lane);
@@ -1660,10 +1673,16 @@ static cudaError_t set_sort_attributes() {
 		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, false, bbLarge>, attr, bytes);
 		if(e == cudaSuccess) e = cudaFuncSetAttribute(sort_kernel<VM, true, bbLarge>, attr, bytes);
 	}
-	if constexpr(VM != kKeysLarge) {
-		if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
-		if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
-	}
+	return e;
+}
+
+// The segmented passes' kernels of a value mode (kSegIndex, 0, kSegOne, 2..6).
+template<int VM>
+static cudaError_t set_seg_attributes() {
+	const int bytes = (int)SortLayout<VM>::kBytes;
+	const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+	cudaError_t e = cudaFuncSetAttribute(seg_sort_kernel<VM, false>, attr, bytes);
+	if(e == cudaSuccess) e = cudaFuncSetAttribute(seg_sort_kernel<VM, true>, attr, bytes);
 	return e;
 }
 
@@ -1692,6 +1711,14 @@ cudaError_t configure_kernels() {
 	if((r = set_sort_attributes<4>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<5>()) != cudaSuccess) e = r;
 	if((r = set_sort_attributes<6>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<kSegIndex>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<0>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<kSegOne>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<2>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<3>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<4>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<5>()) != cudaSuccess) e = r;
+	if((r = set_seg_attributes<6>()) != cudaSuccess) e = r;
 	if((r = configure_onesweep_kernels()) != cudaSuccess) e = r;
 	if((r = configure_coop_kernels()) != cudaSuccess) e = r;
 	if((r = configure_small_array_kernels()) != cudaSuccess) e = r;
@@ -1703,6 +1730,8 @@ cudaError_t configure_kernels() {
 int pass_tile_elements(int valueMode) {
 	switch(valueMode) {
 		case kKeysLarge: return SortLayout<kKeysLarge>::TILE;
+		case kSegOne: return SortLayout<kSegOne>::TILE;
+		case kSegIndex: return SortLayout<kSegIndex>::TILE;
 		case -1: return SortLayout<-1>::TILE;
 		case 0: return SortLayout<0>::TILE;
 		case 1: return SortLayout<1>::TILE;
@@ -2104,8 +2133,8 @@ struct SegScratch {
 };
 
 // The smallest tile of any value mode: the most ranges a plan can cut.
-constexpr int kMinTile = std::min({SortLayout<-1>::TILE, SortLayout<0>::TILE,
-	SortLayout<1>::TILE, SortLayout<2>::TILE, SortLayout<3>::TILE, SortLayout<4>::TILE,
+constexpr int kMinTile = std::min({SortLayout<kSegIndex>::TILE, SortLayout<kSegOne>::TILE,
+	SortLayout<0>::TILE, SortLayout<2>::TILE, SortLayout<3>::TILE, SortLayout<4>::TILE,
 	SortLayout<5>::TILE, SortLayout<6>::TILE});
 
 // Ranges of a plan: a large segment (more than 4096 elements) of t tiles gets
@@ -2145,6 +2174,12 @@ static SegScratch seg_scratch(void* base, int n, int numSegments) {
 	return x;
 }
 
+// The tile class of a segmented pass: index mode and one value array take
+// the segmented sort's own shape.
+static int seg_class(int valueMode) {
+	return valueMode == 1 ? kSegOne : valueMode == kValueIndex ? kSegIndex : valueMode;
+}
+
 cudaError_t launch_seg_plan(const int* offsets, int numSegments, int n,
 	int valueMode, void* scratch, Control* ctrl, volatile unsigned* hostError,
 	cudaStream_t stream) {
@@ -2153,7 +2188,7 @@ cudaError_t launch_seg_plan(const int* offsets, int numSegments, int n,
 	a.offsets = offsets;
 	a.numSegments = numSegments;
 	a.n = n;
-	a.tile = pass_tile_elements(valueMode);
+	a.tile = pass_tile_elements(seg_class(valueMode));
 	a.tinyList = x.tinyList;
 	a.smallList = x.smallList;
 	a.largeList = x.largeList;
@@ -2262,10 +2297,10 @@ cudaError_t launch_seg_pass(const PassBuffers& buf, int valueMode, int pass,
 	a.work = kSegWork + 2 * pass + 1;
 	a.rangeStart = x.rangeStart;
 	a.rangeTrivial = x.rangeTrivial;
-	switch(valueMode) {
-		case -1: return launch_seg_sort_vm<-1>(a, numSMs, stream);
+	switch(seg_class(valueMode)) {
+		case kSegIndex: return launch_seg_sort_vm<kSegIndex>(a, numSMs, stream);
+		case kSegOne: return launch_seg_sort_vm<kSegOne>(a, numSMs, stream);
 		case 0: return launch_seg_sort_vm<0>(a, numSMs, stream);
-		case 1: return launch_seg_sort_vm<1>(a, numSMs, stream);
 		case 2: return launch_seg_sort_vm<2>(a, numSMs, stream);
 		case 3: return launch_seg_sort_vm<3>(a, numSMs, stream);
 		case 4: return launch_seg_sort_vm<4>(a, numSMs, stream);

@@ -123,6 +123,21 @@
 #ifndef MGPU_SORT_SINGLE_MIN_BLOCKS
 #define MGPU_SORT_SINGLE_MIN_BLOCKS 2
 #endif
+// The segmented sort's range passes with index mode or one value array: the
+// single class's earlier shape, which is faster on their short ranges (10k
+// lognormal segments: 36.9 against 36.3 Gkeys/s with 256 x 32).
+#ifndef MGPU_SORT_SEG_SINGLE_THREADS
+#define MGPU_SORT_SEG_SINGLE_THREADS 384
+#endif
+#ifndef MGPU_SORT_SEG_SINGLE_ITEMS
+#define MGPU_SORT_SEG_SINGLE_ITEMS 20
+#endif
+#ifndef MGPU_SORT_SEG_SINGLE_MIN_BLOCKS
+#define MGPU_SORT_SEG_SINGLE_MIN_BLOCKS 2
+#endif
+#ifndef MGPU_SORT_SEG_SINGLE_RANK_BATCH
+#define MGPU_SORT_SEG_SINGLE_RANK_BATCH 10
+#endif
 #ifndef MGPU_SORT_MULTI_THREADS
 #define MGPU_SORT_MULTI_THREADS 768
 #endif
