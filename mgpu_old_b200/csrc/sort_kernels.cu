@@ -359,13 +359,14 @@ struct SortArgs {
 constexpr int kNumBars = 8;
 constexpr int kFaultBar = 7;
 
-// Tile shapes (tile_config.h, chosen by the autotuner). What the
-// measurements showed: larger tiles give each digit longer runs per tile,
-// so fewer partially written sectors reach DRAM; for keys, indices and one
-// value array two CTAs of 384 x 20 per SM were best (256 x 20 with three
-// CTAs per SM was 2% faster at 32 Mi skewed keys but 29% slower at 64 Mi
-// uniform keys: more ranges, more write fronts; one CTA per SM lost the
-// overlap of one CTA's ranking with the other's stores). Several value
+// Tile shapes (tile_config.h, chosen by the autotuner and later sweeps).
+// What the measurements showed: larger tiles give each digit longer runs
+// per tile, so fewer partially written sectors reach DRAM; for indices and
+// one value array two CTAs of 256 x 32 per SM are best (fewer, longer warps:
+// less per-tile work per key than 384 x 20; 256 x 20 with three CTAs per SM
+// was 29% slower at 64 Mi uniform keys: more ranges, more write fronts; one
+// CTA per SM lost the overlap of one CTA's ranking with the other's
+// stores). Several value
 // arrays multiply the write fronts (ranges x digits x arrays), and a front
 // is revisited only once per tile of its range, so partial sectors leave L2
 // before they are completed: one CTA of 768 x 8 per SM halves the ranges.
