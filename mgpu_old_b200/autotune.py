@@ -54,6 +54,13 @@ CLASSES = {
                        (384, 16, 2), (256, 24, 2), (768, 10, 1)],
         "workloads": [("pairs_and24", 1 << 25), ("pairs_u32", 1 << 26), ("index_u32", 1 << 24)],
     },
+    # The segmented sort's range passes with index mode or one value array.
+    "seg_single": {
+        "keys": ("MGPU_SORT_SEG_SINGLE_THREADS", "MGPU_SORT_SEG_SINGLE_ITEMS",
+                 "MGPU_SORT_SEG_SINGLE_MIN_BLOCKS"),
+        "candidates": [(384, 20, 2), (256, 32, 2), (512, 14, 2), (256, 24, 2)],
+        "workloads": [("segments_lognormal", 10_000)],
+    },
     "multi": {
         "keys": ("MGPU_SORT_MULTI_THREADS", "MGPU_SORT_MULTI_ITEMS",
                  "MGPU_SORT_MULTI_MIN_BLOCKS"),
